@@ -1,0 +1,127 @@
+/* C ABI of the B200 Pfaffian-backflow VMC hot path (libnh_b200.so).
+ *
+ * Every entry point takes raw device pointers, sizes and a CUDA stream (as void*), returns an
+ * int status (NH_OK = 0, negative on error; nh_last_error() gives the message of the calling
+ * thread) and never synchronises the host unless its comment says so.  The caller owns every
+ * buffer.  Entry points that need scratch memory take (workspace, workspace_bytes) and have a
+ * *_workspace_bytes() query.  Configurations are int8 +-1 arrays of length 2N (spin-up sites
+ * first, site index x * Ly + y), as in the reference's quantax convention.
+ *
+ * Reference interfaces replaced (paths inside the ChenAo-Phys/NeuralHubbard tree):
+ *   nh_build_wtilde      <- code/backflow/pf_kernel.py:107-124   build_wtilde(W, theta, geom)
+ *   nh_pairing_occ       <- code/backflow/pf_kernel.py:335-351   pairing_occ(Y, idx, Wt, geom)
+ *   nh_slogpf            <- code/backflow/models.py:210          fermix.slogpf(F)
+ *   nh_cnn_forward       <- code/backflow/models.py:163-167      PfaffianBackflow.features(s)
+ *   nh_amplitude         <- code/backflow/models.py:208-211 and code/states.py:318-320
+ *                           quantax Variational.__call__(spins) -> LogArray (sign, logabs)
+ *   nh_local_energy      <- code/quick_start.py:33               H.Oloc(state, Samples(spins, psi))
+ *   nh_metropolis_steps  <- code/states.py:397-408               ParticleHop ... sweep()
+ */
+#ifndef NH_B200_H
+#define NH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NH_ABI_VERSION 1
+
+enum {
+  NH_OK = 0,
+  NH_ERR_INVALID = -1,     /* bad shape, null pointer or inconsistent argument */
+  NH_ERR_UNSUPPORTED = -2, /* size outside what the kernels support */
+  NH_ERR_CUDA = -3,        /* launch or runtime error */
+  NH_ERR_WORKSPACE = -4    /* workspace too small */
+};
+
+/* Per-amplitude status flags (int32 output arrays). */
+enum {
+  NH_FLAG_ZERO_PIVOT = 1,  /* exactly singular pairing block: sign 0, logabs -inf */
+  NH_FLAG_NONFINITE = 2,   /* a non-finite value met during the factorisation */
+  NH_FLAG_GROWTH = 4       /* pivot growth above the threshold (near-nodal configuration) */
+};
+
+/* Parameters of the backflow network (all device pointers, FP32).
+ * conv_w: layers concatenated, layer l of shape (C_out, C_in, 3, 3) (C_in = 2 for l = 0, else
+ *         channels); conv_b: layers concatenated, (channels,) each.  The features are the last
+ *         layer's channels: [0, d) spin up, [d, 2d) spin down, d = channels / 2.
+ * Wt:     (4, N, d) spin-block table from nh_build_wtilde, blocks [uu, ud, du, dd]. */
+typedef struct {
+  const float* conv_w;
+  const float* conv_b;
+  const float* Wt;
+  int32_t Lx, Ly;
+  int32_t n_up, n_dn;
+  int32_t channels;
+  int32_t layers;
+} nh_backflow_params;
+
+/* Hubbard model H = -sum t_ij c+_i c_j + U sum n_up n_dn; n_dirs = 4 (nearest) or 8
+ * (nearest and next-nearest). */
+typedef struct {
+  double t, tp, U;
+  int32_t n_dirs;
+} nh_hubbard_params;
+
+int nh_abi_version(void);
+const char* nh_last_error(void);
+
+/* Wt (4, N, d) from W (3, N, d) = [W_ud, V_uu, V_dd] and theta. */
+int nh_build_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, void* stream);
+
+/* Features y (batch, 2, N, d) of batch configurations (no symmetry image). */
+int nh_cnn_forward(const int8_t* spins, int batch, const nh_backflow_params* p, float* features,
+                   void* stream);
+
+/* Occupied pairing block F (batch, n, n), exactly antisymmetric:
+ * F[p, q] = sum_a Y[p, a] Wt[2 s_p + s_q, r(p, q), a] Y[q, a], idx the ascending occupied modes. */
+int nh_pairing_occ(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
+                   int n, int batch, float* F, void* stream);
+
+/* sign and log|pf| of batch antisymmetric n x n FP32 matrices (n even, n <= 256). */
+int nh_slogpf(const float* F, int n, int batch, float* sign, double* logabs, int32_t* flags,
+              void* stream);
+
+/* Amplitudes of batch configurations.  n_symm = 1: psi(s); n_symm = 8: the projection onto the
+ * trivial representation of Flip(0) Flip(1) SpinInverse, psi_P(s) = 1/8 sum_g eta_g psi(g s). */
+size_t nh_amplitude_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p);
+int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_params* p,
+                 float* sign, double* logabs, int32_t* flags, void* workspace,
+                 size_t workspace_bytes, void* stream);
+
+/* Local energies E_loc (batch,) FP64 of configurations with amplitudes (sign, logabs).  The
+ * connected configurations are evaluated in chunks of at most chunk_configs configurations
+ * (0 = default).  Synchronises the stream once to read the number of connections. */
+size_t nh_local_energy_workspace_bytes(int batch, int n_symm, int chunk_configs,
+                                       const nh_backflow_params* p);
+int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs, int batch,
+                    int n_symm, const nh_backflow_params* p, const nh_hubbard_params* h,
+                    int chunk_configs, double* eloc, int64_t* n_conn_out, void* workspace,
+                    size_t workspace_bytes, void* stream);
+
+/* Connection list of batch configurations: counts (batch,) int32 and, when rec is not null,
+ * records (total,) of (from_mode, to_mode) int32 pairs and matrix elements hval (total,) in
+ * enumeration order (ascending occupied mode, then hop direction). offsets (batch + 1,) int64
+ * are written by the call.  A pure bookkeeping entry point, used by tests. */
+int nh_hop_list(const int8_t* spins, int batch, int Lx, int Ly, const nh_hubbard_params* h,
+                int32_t* counts, int64_t* offsets, int32_t* rec, double* hval, void* stream);
+
+/* nsteps plain Metropolis hop steps (uniform electron, uniform direction, null move when
+ * the target is occupied) on every chain, updating spins, sign and logabs in place.
+ * Random numbers: Philox4x32-10, key (seed_lo, seed_hi), counter (step_lo, chain, 0, step_hi)
+ * for step = step0 + t; draws: x -> electron rank, y -> direction, z -> acceptance uniform.
+ * accepted (batch,) int32 is incremented per accepted move. */
+size_t nh_metropolis_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p);
+int nh_metropolis_steps(int8_t* spins, float* sign, double* logabs, int batch, int n_symm,
+                        const nh_backflow_params* p, int n_dirs, uint64_t seed, int64_t step0,
+                        int nsteps, int32_t* accepted, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NH_B200_H */

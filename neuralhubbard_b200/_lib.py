@@ -1,0 +1,106 @@
+"""ctypes binding of libnh_b200.so (the C ABI declared in include/nh_b200.h).
+
+The library is loaded from this package directory.  There is no fallback: if the shared
+object is missing or fails to load, every operation raises ``NativeLibraryError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnh_b200.so")
+
+NH_OK = 0
+FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH = 1, 2, 4
+
+c_void_p, c_int, c_int64, c_uint64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64
+c_float, c_double, c_size_t = ctypes.c_float, ctypes.c_double, ctypes.c_size_t
+
+
+class NativeLibraryError(RuntimeError):
+    """The CUDA library is missing, failed to load, or an entry point returned an error."""
+
+
+class BackflowParams(ctypes.Structure):
+    _fields_ = [
+        ("conv_w", c_void_p),
+        ("conv_b", c_void_p),
+        ("Wt", c_void_p),
+        ("Lx", ctypes.c_int32),
+        ("Ly", ctypes.c_int32),
+        ("n_up", ctypes.c_int32),
+        ("n_dn", ctypes.c_int32),
+        ("channels", ctypes.c_int32),
+        ("layers", ctypes.c_int32),
+    ]
+
+
+class HubbardParams(ctypes.Structure):
+    _fields_ = [("t", c_double), ("tp", c_double), ("U", c_double), ("n_dirs", ctypes.c_int32)]
+
+
+P_BF = ctypes.POINTER(BackflowParams)
+P_H = ctypes.POINTER(HubbardParams)
+
+# name -> (restype, argtypes); every symbol declared in include/nh_b200.h.
+SIGNATURES = {
+    "nh_abi_version": (c_int, []),
+    "nh_last_error": (ctypes.c_char_p, []),
+    "nh_build_wtilde": (c_int, [c_void_p, c_float, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "nh_cnn_forward": (c_int, [c_void_p, c_int, P_BF, c_void_p, c_void_p]),
+    "nh_pairing_occ": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int,
+                               c_void_p, c_void_p]),
+    "nh_slogpf": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "nh_amplitude_workspace_bytes": (c_size_t, [c_int, c_int, P_BF]),
+    "nh_amplitude": (c_int, [c_void_p, c_int, c_int, P_BF, c_void_p, c_void_p, c_void_p,
+                             c_void_p, c_size_t, c_void_p]),
+    "nh_local_energy_workspace_bytes": (c_size_t, [c_int, c_int, c_int, P_BF]),
+    "nh_local_energy": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, P_BF, P_H, c_int,
+                                c_void_p, ctypes.POINTER(c_int64), c_void_p, c_size_t, c_void_p]),
+    "nh_hop_list": (c_int, [c_void_p, c_int, c_int, c_int, P_H, c_void_p, c_void_p, c_void_p,
+                            c_void_p, c_void_p]),
+    "nh_metropolis_workspace_bytes": (c_size_t, [c_int, c_int, P_BF]),
+    "nh_metropolis_steps": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, P_BF, c_int,
+                                    c_uint64, c_int64, c_int, c_void_p, c_void_p, c_size_t,
+                                    c_void_p]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load (once) and return the library with its argument types set."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise NativeLibraryError(
+                f"{LIB_PATH} is missing; build it with `python -m neuralhubbard_b200.build`")
+        try:
+            lib = ctypes.CDLL(LIB_PATH)
+        except OSError as e:
+            raise NativeLibraryError(f"cannot load {LIB_PATH}: {e}") from e
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != NH_OK:
+        msg = load().nh_last_error()
+        raise NativeLibraryError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+
+def call(name: str, *args):
+    """Call an int-returning entry point and raise on a non-zero status."""
+    rc = getattr(load(), name)(*args)
+    check(rc, name)
+    return rc

@@ -1,0 +1,176 @@
+"""Pfaffian backflow model and its operators on the GPU (host side of the C ABI).
+
+Mirrors the reference's operator surface:
+
+* ``PairGeometry``        <- ``code/backflow/pf_kernel.py:58-77``
+* ``build_wtilde``        <- ``code/backflow/pf_kernel.py:107-124``
+* ``pairing_occ``         <- ``code/backflow/pf_kernel.py:335-351`` (forward only)
+* ``slogpf``              <- ``fermix.slogpf`` as called at ``code/backflow/models.py:210``
+* ``PfaffianBackflow``    <- ``code/backflow/models.py:121-211`` with the backflow CNN of the
+                             graded configurations (4 periodic 3x3 layers, 32 channels,
+                             tanh-GELU between layers, 2-channel +-1 input).
+
+Every computation runs in libnh_b200.so; tensors are torch CUDA tensors used for device memory
+and streams only.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import NamedTuple, Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+class PairGeometry(NamedTuple):
+    """Static description of the pairing problem (``pf_kernel.py:58-77``)."""
+
+    LX: int
+    LY: int
+    d: int
+    n_up: int
+    n_dn: int
+
+    @property
+    def N(self) -> int:
+        return self.LX * self.LY
+
+    @property
+    def n_occ(self) -> int:
+        return self.n_up + self.n_dn
+
+
+def stream_ptr(device=None) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def _require_cuda(t: torch.Tensor, dtype: torch.dtype, name: str) -> torch.Tensor:
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    return t.contiguous()
+
+
+_WS: dict = {}
+
+
+def workspace(nbytes: int, device: torch.device, tag: str = "default") -> torch.Tensor:
+    """A cached byte buffer of at least ``nbytes`` on ``device`` (grown on demand)."""
+    key = (str(device), tag)
+    buf = _WS.get(key)
+    if buf is None or buf.numel() < nbytes:
+        buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+        _WS[key] = buf
+    return buf
+
+
+def init_params(Lx: int, Ly: int, channels: int = 32, layers: int = 4, std: float = 0.02,
+                seed: int = 0) -> dict:
+    """Seeded random parameters (numpy FP32): conv weights and biases N(0, std), the pairing
+    parameters W (3, N, d) N(0, 1) / sqrt(d) and theta = 0.55 (``models.py:146-149``)."""
+    rng = np.random.default_rng(seed)
+    conv_w, conv_b = [], []
+    cin = 2
+    for _ in range(layers):
+        conv_w.append(rng.normal(0.0, std, (channels, cin, 3, 3)).astype(np.float32))
+        conv_b.append(rng.normal(0.0, std, (channels,)).astype(np.float32))
+        cin = channels
+    d = channels // 2
+    W = (rng.normal(0.0, 1.0, (3, Lx * Ly, d)) / np.sqrt(d)).astype(np.float32)
+    return dict(conv_w=conv_w, conv_b=conv_b, W=W, theta=np.float32(0.55), Lx=Lx, Ly=Ly)
+
+
+def build_wtilde(W: torch.Tensor, theta: float, geom: PairGeometry) -> torch.Tensor:
+    """(3, N, d) -> (4, N, d) spin-block table with the distance envelope."""
+    W = _require_cuda(W, torch.float32, "W")
+    if tuple(W.shape) != (3, geom.N, geom.d):
+        raise ValueError(f"W shape {tuple(W.shape)} != (3, {geom.N}, {geom.d})")
+    Wt = torch.empty((4, geom.N, geom.d), dtype=torch.float32, device=W.device)
+    _lib.call("nh_build_wtilde", W.data_ptr(), float(theta), geom.LX, geom.LY, geom.d,
+              Wt.data_ptr(), stream_ptr(W.device))
+    return Wt
+
+
+def pairing_occ(Y: torch.Tensor, idx: torch.Tensor, Wt: torch.Tensor, geom: PairGeometry) -> torch.Tensor:
+    """F (..., n, n) = sum_a Y[p, a] Wt[2 s_p + s_q, site_p - site_q, a] Y[q, a], exactly
+    antisymmetric; Y (..., n, d) FP32, idx (..., n) int32 ascending occupied modes."""
+    Y = _require_cuda(Y, torch.float32, "Y")
+    idx = _require_cuda(idx, torch.int32, "idx")
+    Wt = _require_cuda(Wt, torch.float32, "Wt")
+    n, d = Y.shape[-2], Y.shape[-1]
+    if d != geom.d or idx.shape[-1] != n or tuple(Wt.shape) != (4, geom.N, d):
+        raise ValueError("pairing_occ: inconsistent shapes")
+    batch = int(np.prod(Y.shape[:-2])) if Y.dim() > 2 else 1
+    F = torch.empty(Y.shape[:-2] + (n, n), dtype=torch.float32, device=Y.device)
+    _lib.call("nh_pairing_occ", Y.data_ptr(), idx.data_ptr(), Wt.data_ptr(), geom.LX, geom.LY, d,
+              n, batch, F.data_ptr(), stream_ptr(Y.device))
+    return F
+
+
+def slogpf(F: torch.Tensor):
+    """(sign FP32, logabs FP64, flags int32) of the Pfaffians of antisymmetric F (..., n, n)
+    in FP32; only the strict lower triangle is read."""
+    F = _require_cuda(F, torch.float32, "F")
+    n = F.shape[-1]
+    if F.shape[-2] != n:
+        raise ValueError("slogpf: matrices must be square")
+    batch_shape = F.shape[:-2]
+    batch = int(np.prod(batch_shape)) if len(batch_shape) else 1
+    sign = torch.empty(batch, dtype=torch.float32, device=F.device)
+    logabs = torch.empty(batch, dtype=torch.float64, device=F.device)
+    flags = torch.empty(batch, dtype=torch.int32, device=F.device)
+    _lib.call("nh_slogpf", F.data_ptr(), n, batch, sign.data_ptr(), logabs.data_ptr(),
+              flags.data_ptr(), stream_ptr(F.device))
+    return sign.reshape(batch_shape), logabs.reshape(batch_shape), flags.reshape(batch_shape)
+
+
+class PfaffianBackflow:
+    """psi(s) = pf[n * f(n) * n] * fermion_inverse_sign(s) (``models.py:121-211``) with the
+    backflow CNN of the graded configurations; parameters live on the GPU in FP32."""
+
+    def __init__(self, Lx: int, Ly: int, n_up: int, n_dn: int, params: Optional[dict] = None,
+                 channels: int = 32, layers: int = 4, seed: int = 0, device="cuda"):
+        self.device = torch.device(device)
+        if params is None:
+            params = init_params(Lx, Ly, channels, layers, seed=seed)
+        self.channels = int(params["conv_w"][0].shape[0])
+        self.layers = len(params["conv_w"])
+        self.geom = PairGeometry(Lx, Ly, self.channels // 2, n_up, n_dn)
+        self.host_params = params
+        self.set_params(params)
+
+    def set_params(self, params: dict) -> None:
+        dev = self.device
+        self.conv_w = torch.from_numpy(np.concatenate(
+            [np.asarray(w, np.float32).ravel() for w in params["conv_w"]])).to(dev)
+        self.conv_b = torch.from_numpy(np.concatenate(
+            [np.asarray(b, np.float32).ravel() for b in params["conv_b"]])).to(dev)
+        self.W = torch.from_numpy(np.asarray(params["W"], np.float32)).to(dev).contiguous()
+        self.theta = float(params["theta"])
+        self.Wt = build_wtilde(self.W, self.theta, self.geom)
+        self.host_params = params
+
+    def c_params(self) -> _lib.BackflowParams:
+        g = self.geom
+        return _lib.BackflowParams(self.conv_w.data_ptr(), self.conv_b.data_ptr(),
+                                   self.Wt.data_ptr(), g.LX, g.LY, g.n_up, g.n_dn, self.channels,
+                                   self.layers)
+
+    def features(self, spins: torch.Tensor) -> torch.Tensor:
+        """(B, 2, N, d) backflow features of int8 configurations (B, 2N)."""
+        spins = _require_cuda(spins, torch.int8, "spins")
+        B = spins.shape[0]
+        out = torch.empty((B, 2, self.geom.N, self.geom.d), dtype=torch.float32,
+                          device=spins.device)
+        p = self.c_params()
+        _lib.call("nh_cnn_forward", spins.data_ptr(), B, ctypes.byref(p), out.data_ptr(),
+                  stream_ptr(spins.device))
+        return out

@@ -1,0 +1,141 @@
+// Internal declarations shared by the CUDA sources of libnh_b200.so (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/nh_b200.h"
+
+namespace nh {
+
+constexpr int kNumThreads = 256;  // block size of every per-item kernel
+constexpr int kMaxN = 1024;       // sites per lattice supported by the bookkeeping kernels
+
+// ------------------------------------------------------------------ host-side error state
+void set_error(const char* fmt, ...);
+int fail(int code, const char* fmt, ...);
+int check_cuda(cudaError_t e, const char* what);
+int check_launch(const char* what);
+
+// ------------------------------------------------------------------ lattice helpers
+// Mode m = sigma * N + x * Ly + y.  Symmetry element g = fx + 2 fy + 4 si:
+// Flip(axis=0) x -> -x mod Lx, Flip(axis=1) y -> -y mod Ly, SpinInverse swaps sigma.
+__host__ __device__ __forceinline__ int sym_map(int m, int g, int Lx, int Ly, int N) {
+  int sigma = m >= N ? 1 : 0;
+  int site = m - sigma * N;
+  int x = site / Ly;
+  int y = site - x * Ly;
+  if (g & 1) x = x ? Lx - x : 0;
+  if (g & 2) y = y ? Ly - y : 0;
+  if (g & 4) sigma ^= 1;
+  return sigma * N + x * Ly + y;
+}
+
+// Hop directions: (1,0), (-1,0), (0,1), (0,-1), (1,1), (1,-1), (-1,1), (-1,-1).
+__host__ __device__ __forceinline__ int hop_target_site(int site, int dir, int Lx, int Ly) {
+  const int dxs[8] = {1, -1, 0, 0, 1, 1, -1, -1};
+  const int dys[8] = {0, 0, 1, -1, 1, -1, 1, -1};
+  int x = site / Ly;
+  int y = site - x * Ly;
+  x += dxs[dir];
+  y += dys[dir];
+  x = x < 0 ? x + Lx : (x >= Lx ? x - Lx : x);
+  y = y < 0 ? y + Ly : (y >= Ly ? y - Ly : y);
+  return x * Ly + y;
+}
+
+// ------------------------------------------------------------------ Philox4x32-10
+// Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC'11).
+struct u32x4 {
+  uint32_t x, y, z, w;
+};
+
+__host__ __device__ __forceinline__ u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    c = u32x4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// u = (x >> 8) * 2^-24, exact in FP32 and FP64.
+__host__ __device__ __forceinline__ double u32_to_unit(uint32_t x) {
+  return (double)(x >> 8) * (1.0 / 16777216.0);
+}
+
+// ------------------------------------------------------------------ amplitude pipeline
+// A "configuration" c is spins[sample(c)] with an optional hop from(c) -> to(c) applied;
+// an "item" is (configuration c, symmetry image g), item = c * G + g.
+struct ConfigList {
+  const int8_t* spins;       // (n_samples, 2N)
+  const int32_t* sample;     // (n_cfg,) sample of each configuration, null: c itself
+  const int32_t* from;       // (n_cfg,) hop source mode or -1, null: no hop
+  const int32_t* to;         // (n_cfg,) hop target mode
+  const int32_t* n_cfg_dev;  // device count (overrides n_cfg when not null)
+  int n_cfg;                 // host count (upper bound when n_cfg_dev is set)
+  int G;                     // images per configuration: 1 or 8
+};
+
+struct PipelineBuffers {
+  float* Y;           // (items, n, d)
+  int32_t* idx;       // (items, n)
+  float* item_sign;   // (items,)
+  float* pf_sign;     // (items,)
+  double* pf_logabs;  // (items,)
+  int32_t* pf_flags;  // (items,)
+};
+
+size_t pipeline_bytes(int max_items, int n, int d);
+PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d);
+
+// Launchers (return NH_OK or an error code).
+int launch_cnn(const ConfigList& cl, const nh_backflow_params& p, int out_mode, float* feat,
+               float* Y, int32_t* idx, float* item_sign, cudaStream_t st);
+int launch_pfaffian_from_F(const float* F, int n, int batch, float* sign, double* logabs,
+                           int32_t* flags, cudaStream_t st);
+int launch_pfaffian_gather(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly,
+                           int d, int n, int max_items, const ConfigList* cl,
+                           const float* item_sign, float* sign, double* logabs, int32_t* flags,
+                           cudaStream_t st);
+int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
+                   int n, int batch, float* F, cudaStream_t st);
+int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, int n_cfg,
+                   const int32_t* n_cfg_dev, float* sign, double* logabs, int32_t* flags,
+                   cudaStream_t st);
+int launch_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, cudaStream_t st);
+
+// Full amplitude of a configuration list: CNN -> gather + Pfaffian -> image combination.
+int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const PipelineBuffers& b,
+                 float* sign, double* logabs, int32_t* flags, cudaStream_t st);
+
+// Hops / local energy / sampler.
+int launch_hop_count(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs,
+                     int32_t* counts, cudaStream_t st);
+int launch_scan_counts(const int32_t* counts, int batch, int64_t* offsets, cudaStream_t st);
+int launch_hop_emit(const int8_t* spins, int batch, int Lx, int Ly, const nh_hubbard_params& h,
+                    const int64_t* offsets, int32_t* rec, double* hval, int32_t* owner,
+                    int32_t* from, int32_t* to, cudaStream_t st);
+int launch_eloc_reduce(const int8_t* spins, const float* sign, const double* logabs, int batch,
+                       int N, double U, const int64_t* offsets, const double* hval,
+                       const float* csign, const double* clogabs, double* eloc,
+                       cudaStream_t st);
+int launch_mh_propose(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs,
+                      uint64_t seed, int64_t step, int32_t* valid, int32_t* from, int32_t* to,
+                      cudaStream_t st);
+int launch_compact(const int32_t* valid, const int32_t* from, const int32_t* to, int batch,
+                   int32_t* c_sample, int32_t* c_from, int32_t* c_to, int32_t* c_count,
+                   cudaStream_t st);
+int launch_mh_accept(int8_t* spins, float* sign, double* logabs, int batch, int N,
+                     const int32_t* c_sample, const int32_t* c_from, const int32_t* c_to,
+                     const int32_t* c_count, const float* psign, const double* plogabs,
+                     uint64_t seed, int64_t step, int32_t* accepted, cudaStream_t st);
+
+int num_sms();
+
+}  // namespace nh

@@ -1,0 +1,99 @@
+"""Host-side checks that need no GPU: the C-ABI library loads and exports every symbol of
+include/nh_b200.h, the ctypes table matches the header, and the chain-parallel statistics work
+across two gloo ranks."""
+
+import ctypes
+import os
+import re
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "nh_b200.h")
+LIB = os.path.join(ROOT, "neuralhubbard_b200", "libnh_b200.so")
+
+
+def header_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nh_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_header_symbol():
+    if not os.path.exists(LIB):
+        pytest.skip("libnh_b200.so not built")
+    lib = ctypes.CDLL(LIB)  # loads without a GPU: no compute call is made
+    syms = header_symbols()
+    assert len(syms) >= 13
+    for s in syms:
+        assert hasattr(lib, s), s
+    lib.nh_abi_version.restype = ctypes.c_int
+    assert lib.nh_abi_version() == 1
+
+
+def test_ctypes_table_matches_header():
+    from neuralhubbard_b200 import _lib
+
+    assert sorted(_lib.SIGNATURES) == header_symbols()
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    from neuralhubbard_b200 import _lib
+
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "absent.so"))
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(_lib.NativeLibraryError):
+        _lib.load()
+
+
+def test_shard_chains_cover():
+    from neuralhubbard_b200.distributed import shard_chains
+
+    for n, w in [(10, 3), (8192, 8), (5, 8)]:
+        parts = [shard_chains(n, r, w) for r in range(w)]
+        assert sum(c for _, c in parts) == n
+        assert all(parts[r][0] + parts[r][1] == parts[r + 1][0] for r in range(w - 1))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from neuralhubbard_b200.distributed import energy_stats, shard_chains
+
+    rng = np.random.default_rng(0)
+    e_all = torch.from_numpy(rng.normal(-0.7, 0.1, 1000))
+    s, c = shard_chains(1000, rank, world)
+    st = energy_stats(e_all[s : s + c], N=1)
+    out[rank] = (st["E_per_site"], st["var_per_site"], st["count"])
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_energy_stats_gloo_two_ranks():
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    e_all = np.random.default_rng(0).normal(-0.7, 0.1, 1000)
+    for r in range(2):
+        m, v, n = out[r]
+        assert n == 1000
+        assert m == pytest.approx(e_all.mean(), abs=1e-12)
+        assert v == pytest.approx(e_all.var(), rel=1e-9)
