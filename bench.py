@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Benchmark of the Pfaffian-backflow amplitude path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one projected-amplitude call ``state(spins)`` on the 16x16 lattice (N = 256,
+112 + 112 electrons, 224 x 224 Pfaffians) for 8192 configurations x 8 symmetry images =
+65,536 amplitudes, with seeded N(0, 0.02) weights of the 4-layer, 32-channel backflow CNN and
+synthetic uniformly random configurations (no dataset is involved).  ``value`` is amplitude
+evaluations per second over all ranks with the inputs resident in HBM; ``e2e`` is the same
+metric through the public API with the configurations copied from pinned host memory and the
+amplitudes read back every step.
+
+Under torchrun each rank evaluates its own 8192 configurations (weak scaling); the time is the
+maximum over ranks of the summed per-step CUDA-event durations.  ``--impl reference`` times the
+CPU restatement of the same path (the reference's JAX stack cannot be installed here) on all
+host cores, on rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "effective samples/s + amplitude evals/s, 16x16 Pfaffian; chosen vs plain, 1 B200"
+UNIT = "amplitude evals/s"
+L, NE, BATCH, IMAGES, CHANNELS, LAYERS = 16, 112, 8192, 8, 32, 4
+N_SITES = L * L
+N_OCC = 2 * NE
+D_FEAT = CHANNELS // 2
+# Algorithmic work per amplitude (one image): CNN 2 * 9 * (2*32 + 3*32*32) FLOP per site,
+# occupied gather 2 n^2 d, Pfaffian n^3 / 3 (the Table S3 convention of the reference).
+CNN_FLOP = 2 * 9 * (2 * CHANNELS + (LAYERS - 1) * CHANNELS * CHANNELS) * N_SITES
+GATHER_FLOP = 2 * N_OCC * N_OCC * D_FEAT
+PFAFFIAN_FLOP = N_OCC ** 3 / 3.0
+FP32_CORE_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FMA rate of the CUDA cores
+# DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum), keyed by
+# kernel; filled from the committed summaries under profiles/.  None until captured.
+TRAFFIC_BYTES = {"pfaffian": None, "cnn": None}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU restatement (oracle)
+
+def _cpu_worker(args):
+    spins, params = args
+    from oracle import projection
+
+    t0 = time.perf_counter()
+    projection.projected_amplitude(spins, params, symm=True)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(target_s: float = 12.0) -> dict:
+    """Projected amplitudes of the same workload by the CPU restatement, all host cores in a
+    spawn pool (one numpy thread each), on a bounded sample sized for ~target_s seconds."""
+    import multiprocessing as mp
+
+    from neuralhubbard_b200.backflow import init_params
+    from neuralhubbard_b200.sampler import random_spins
+
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except Exception:
+        cores = os.cpu_count() or 1
+    p = init_params(L, L, CHANNELS, LAYERS, seed=0)
+    params = dict(conv_w=[w.astype(np.float64) for w in p["conv_w"]],
+                  conv_b=[b.astype(np.float64) for b in p["conv_b"]],
+                  W=p["W"].astype(np.float64), theta=float(p["theta"]), Lx=L, Ly=L)
+    rng = np.random.default_rng(123)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        one = random_spins(rng, 1, N_SITES, NE, NE)
+        pool.map(_cpu_worker, [(one, params)] * cores)  # warm the workers
+        t_one = max(pool.map(_cpu_worker, [(one, params)] * cores))
+        per_worker = max(1, int(target_s / max(t_one, 1e-3)))
+        jobs = [(random_spins(rng, per_worker, N_SITES, NE, NE), params) for _ in range(cores)]
+        t0 = time.perf_counter()
+        pool.map(_cpu_worker, jobs)
+        wall = time.perf_counter() - t0
+    n_amp = cores * per_worker * IMAGES
+    return {"value": n_amp / wall, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{cores * per_worker} configurations x {IMAGES} images at 16x16 "
+                      f"({n_amp} amplitudes, FP64 numpy restatement, {wall:.1f} s)",
+            "seconds": wall}
+
+
+# ---------------------------------------------------------------- GPU arm
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    import neuralhubbard_b200 as nh
+    from neuralhubbard_b200 import _lib
+    from neuralhubbard_b200.distributed import init_from_env
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    multi = init_from_env("nccl") if world > 1 else False
+
+    params = nh.init_params(L, L, CHANNELS, LAYERS, std=0.02, seed=0)
+    model = nh.PfaffianBackflow(L, L, NE, NE, params=params, device=dev)
+    state = nh.Variational(model, symm=True, max_parallel=BATCH)
+    rng = np.random.default_rng(1000 + rank)
+    spins_host = torch.from_numpy(nh.random_spins(rng, BATCH, N_SITES, NE, NE)).pin_memory()
+    spins = spins_host.to(dev)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    st = torch.cuda.current_stream(dev)
+
+    for _ in range(args.warmup):
+        state(spins)
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    if multi:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    _lib.profile_read()
+    _lib.profile_enable(True)
+    step_ms = []
+    for _ in range(args.steps):
+        flush.fill_(1)  # evict L2 between steps (not timed)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        psi = state(spins)
+        e1.record(st)
+        step_ms.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    _lib.profile_enable(False)
+    kern = _lib.profile_read()
+    if multi:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if multi:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    n_amp = world * BATCH * IMAGES * args.steps
+    value = n_amp / (total_ms / 1e3)
+
+    # e2e: public API, configurations from pinned host memory, amplitudes back to the host
+    sign_h = torch.empty(BATCH, dtype=torch.float32).pin_memory()
+    logabs_h = torch.empty(BATCH, dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    for _ in range(max(2, args.steps // 2)):
+        flush.fill_(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        psi = state(spins_host)
+        sign_h.copy_(psi.sign, non_blocking=True)
+        logabs_h.copy_(psi.logabs, non_blocking=True)
+        e1.record(st)
+        e2e_ms.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    e2e_total = sum(a.elapsed_time(b) for a, b in e2e_ms)
+    te = torch.tensor([e2e_total], dtype=torch.float64, device=dev)
+    if multi:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * BATCH * IMAGES * len(e2e_ms) / (float(te.item()) / 1e3)
+
+    # roofline of the dominant kernel (live CUDA-event durations on the launching stream)
+    hbm, bf16, peak_kind = peaks()
+    dom = max(kern.items(), key=lambda kv: kv[1][0])[0] if kern else None
+    roof = None
+    if dom is not None:
+        ms, launches = kern[dom]
+        per_launch_s = ms / launches / 1e3
+        amps_per_launch = BATCH * IMAGES * args.steps / launches
+        flop = {"cnn": CNN_FLOP, "pfaffian": PFAFFIAN_FLOP + GATHER_FLOP}.get(dom, 0.0)
+        achieved = flop * amps_per_launch / per_launch_s / 1e12
+        tb = TRAFFIC_BYTES.get(dom)
+        roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": bf16,
+                "unit": "TFLOP/s", "frac": achieved / bf16, "traffic": tb,
+                "peak_source": f"{peak_kind} bf16 dense (MEASURED_PEAKS.json)",
+                "fp32_core_frac": achieved / FP32_CORE_PEAK_TFLOPS,
+                "note": "FP32 CUDA-core kernel; fp32_core_frac is against the nominal FP32 FMA "
+                        "rate of 148 SMs at 1965 MHz"}
+    launches = sum(n for _, n in kern.values())
+    kernels = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1]} for k, v in kern.items()}
+
+    if rank == 0:
+        cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": "projected amplitudes, 16x16 Hubbard lattice, 112+112 "
+                                   "electrons, 8192 configurations x 8 images = 65536 "
+                                   "Pfaffians of 224x224 per step",
+                       "form": "plain FP32", "L": L, "batch": BATCH, "images": IMAGES,
+                       "cnn": "4 x periodic 3x3, 32 channels, tanh-GELU, N(0, 0.02)",
+                       "l2": "512 MiB written between timed steps, outside the step events",
+                       "parallelism": f"replicas x{world} (chains data-parallel)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": BATCH * 2 * N_SITES,
+                    "d2h_bytes_per_step": BATCH * (4 + 8)},
+            "roofline": roof, "kernels": kernels, "gpu_launches": launches,
+            "cpu_baseline": cpu, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if multi:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    per_step = [cpu_baseline(target_s=max(2.0, 60.0 / max(1, args.steps + args.warmup)))
+                for _ in range(args.warmup + args.steps)][args.warmup:]
+    secs = sum(p["seconds"] for p in per_step)
+    amps = sum(p["value"] * p["seconds"] for p in per_step)
+    value = amps / secs
+    last = per_step[-1]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+        "data": "synthetic",
+        "config": {"workload": "projected amplitudes, 16x16 Hubbard lattice, 112+112 electrons, "
+                               "8 images per configuration (bounded sample per step)",
+                   "form": "CPU restatement of the reference path (JAX stack not installable)",
+                   "L": L, "images": IMAGES},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": last["cores"], "kind": "port",
+                         "sample": last["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    global BATCH
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch", type=int, default=BATCH,
+                    help="configurations per step (default 8192; smaller only for profiling)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    BATCH = args.batch
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

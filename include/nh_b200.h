@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define NH_ABI_VERSION 1
+#define NH_ABI_VERSION 2
 
 enum {
   NH_OK = 0,
@@ -41,22 +41,34 @@ enum {
 enum {
   NH_FLAG_ZERO_PIVOT = 1,  /* exactly singular pairing block: sign 0, logabs -inf */
   NH_FLAG_NONFINITE = 2,   /* a non-finite value met during the factorisation */
-  NH_FLAG_GROWTH = 4       /* pivot growth above the threshold (near-nodal configuration) */
+  NH_FLAG_GROWTH = 4,      /* pivot ratio above cond_tau (near-nodal, ill-conditioned block) */
+  NH_FLAG_REFINED = 8      /* recomputed in FP64 because of NH_FLAG_GROWTH */
 };
 
-/* Parameters of the backflow network (all device pointers, FP32).
- * conv_w: layers concatenated, layer l of shape (C_out, C_in, 3, 3) (C_in = 2 for l = 0, else
- *         channels); conv_b: layers concatenated, (channels,) each.  The features are the last
- *         layer's channels: [0, d) spin up, [d, 2d) spin down, d = channels / 2.
- * Wt:     (4, N, d) spin-block table from nh_build_wtilde, blocks [uu, ud, du, dd]. */
+/* Parameters of the backflow network (device pointers).
+ * conv_w:        FP32, layers concatenated, layer l of shape (C_out, C_in, 3, 3) (C_in = 2 for
+ *                l = 0, else channels); conv_b: FP32, (channels,) per layer, concatenated.
+ *                The features are the last layer's channels: [0, d) spin up, [d, 2d) spin
+ *                down, d = channels / 2.
+ * conv_w_packed: the same weights repacked by nh_pack_cnn_weights (read by the kernels).
+ * Wt:            FP32 (4, N, d) spin-block table from nh_build_wtilde, blocks [uu, ud, du, dd].
+ * Wt64:          the same table in FP64 (nh_build_wtilde), or null to disable the FP64
+ *                recompute of ill-conditioned items.
+ * cond_tau:      an item whose largest / smallest pivot magnitude exceeds cond_tau is flagged
+ *                NH_FLAG_GROWTH and, when Wt64 is set and the FP64 kernels fit in shared
+ *                memory (n <= 232, N <= 256 at 32 channels), recomputed end to end in FP64
+ *                (CNN, gather, Pfaffian; NH_FLAG_REFINED); <= 0 disables both. */
 typedef struct {
   const float* conv_w;
   const float* conv_b;
+  const float* conv_w_packed;
   const float* Wt;
+  const double* Wt64;
   int32_t Lx, Ly;
   int32_t n_up, n_dn;
   int32_t channels;
   int32_t layers;
+  double cond_tau;
 } nh_backflow_params;
 
 /* Hubbard model H = -sum t_ij c+_i c_j + U sum n_up n_dn; n_dirs = 4 (nearest) or 8
@@ -69,8 +81,41 @@ typedef struct {
 int nh_abi_version(void);
 const char* nh_last_error(void);
 
-/* Wt (4, N, d) from W (3, N, d) = [W_ud, V_uu, V_dd] and theta. */
-int nh_build_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, void* stream);
+/* Per-kernel timing (no counterpart in the reference, whose timing is wall clock around calls,
+ * code/train_pfaffian_16x16_tpm02.py:107,124).  While enabled, every kernel launch of the library
+ * is bracketed by CUDA events on its launching stream.  nh_profile_read waits for the pending
+ * events, writes the accumulated milliseconds and launch counts of each kernel id (< n_ids,
+ * ids NH_K_*), and resets the totals. */
+enum {
+  NH_K_CNN = 0,
+  NH_K_PFAFFIAN = 1,
+  NH_K_PAIRING = 2,
+  NH_K_COMBINE = 3,
+  NH_K_HOP_COUNT = 4,
+  NH_K_SCAN = 5,
+  NH_K_HOP_EMIT = 6,
+  NH_K_ELOC_REDUCE = 7,
+  NH_K_MH_PROPOSE = 8,
+  NH_K_COMPACT = 9,
+  NH_K_MH_ACCEPT = 10,
+  NH_K_WTILDE = 11,
+  NH_K_PFAFFIAN64 = 12,
+  NH_K_CNN64 = 13,
+  NH_K_FLAGGED = 14,
+  NH_K_PACK = 15,
+  NH_K_COUNT = 16
+};
+int nh_profile_enable(int on);
+int nh_profile_read(double* ms, int64_t* launches, int n_ids);
+
+/* Wt (4, N, d) FP32 and, when Wt64 is not null, the same table in FP64, from
+ * W (3, N, d) = [W_ud, V_uu, V_dd] and theta. */
+int nh_build_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, double* Wt64,
+                    void* stream);
+
+/* packed (18 C + 9 C^2 (layers - 1),) = conv_w rearranged per layer as [ci][tap][co]. */
+int nh_pack_cnn_weights(const float* conv_w, int channels, int layers, float* packed,
+                        void* stream);
 
 /* Features y (batch, 2, N, d) of batch configurations (no symmetry image). */
 int nh_cnn_forward(const int8_t* spins, int batch, const nh_backflow_params* p, float* features,
@@ -81,9 +126,13 @@ int nh_cnn_forward(const int8_t* spins, int batch, const nh_backflow_params* p, 
 int nh_pairing_occ(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
                    int n, int batch, float* F, void* stream);
 
-/* sign and log|pf| of batch antisymmetric n x n FP32 matrices (n even, n <= 256). */
-int nh_slogpf(const float* F, int n, int batch, float* sign, double* logabs, int32_t* flags,
-              void* stream);
+/* sign and log|pf| of batch antisymmetric n x n FP32 matrices (n even, n <= 256); only the
+ * strict lower triangle is read.  With cond_tau > 0 the matrices whose pivot ratio exceeds it
+ * are flagged NH_FLAG_GROWTH and factorised again in FP64 (NH_FLAG_REFINED) when n <= 232 (the FP64
+ * triangle must fit in shared memory); the workspace holds the list of those matrices. */
+size_t nh_slogpf_workspace_bytes(int batch);
+int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, double* logabs,
+              int32_t* flags, void* workspace, size_t workspace_bytes, void* stream);
 
 /* Amplitudes of batch configurations.  n_symm = 1: psi(s); n_symm = 8: the projection onto the
  * trivial representation of Flip(0) Flip(1) SpinInverse, psi_P(s) = 1/8 sum_g eta_g psi(g s). */

@@ -14,7 +14,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libnh_b200.so")
 
 NH_OK = 0
-FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH = 1, 2, 4
+FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH, FLAG_REFINED = 1, 2, 4, 8
 
 c_void_p, c_int, c_int64, c_uint64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64
 c_float, c_double, c_size_t = ctypes.c_float, ctypes.c_double, ctypes.c_size_t
@@ -28,13 +28,16 @@ class BackflowParams(ctypes.Structure):
     _fields_ = [
         ("conv_w", c_void_p),
         ("conv_b", c_void_p),
+        ("conv_w_packed", c_void_p),
         ("Wt", c_void_p),
+        ("Wt64", c_void_p),
         ("Lx", ctypes.c_int32),
         ("Ly", ctypes.c_int32),
         ("n_up", ctypes.c_int32),
         ("n_dn", ctypes.c_int32),
         ("channels", ctypes.c_int32),
         ("layers", ctypes.c_int32),
+        ("cond_tau", c_double),
     ]
 
 
@@ -49,11 +52,17 @@ P_H = ctypes.POINTER(HubbardParams)
 SIGNATURES = {
     "nh_abi_version": (c_int, []),
     "nh_last_error": (ctypes.c_char_p, []),
-    "nh_build_wtilde": (c_int, [c_void_p, c_float, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "nh_profile_enable": (c_int, [c_int]),
+    "nh_profile_read": (c_int, [c_void_p, c_void_p, c_int]),
+    "nh_build_wtilde": (c_int, [c_void_p, c_float, c_int, c_int, c_int, c_void_p, c_void_p,
+                                c_void_p]),
+    "nh_pack_cnn_weights": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "nh_cnn_forward": (c_int, [c_void_p, c_int, P_BF, c_void_p, c_void_p]),
     "nh_pairing_occ": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int,
                                c_void_p, c_void_p]),
-    "nh_slogpf": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "nh_slogpf_workspace_bytes": (c_size_t, [c_int]),
+    "nh_slogpf": (c_int, [c_void_p, c_int, c_int, c_double, c_void_p, c_void_p, c_void_p,
+                          c_void_p, c_size_t, c_void_p]),
     "nh_amplitude_workspace_bytes": (c_size_t, [c_int, c_int, P_BF]),
     "nh_amplitude": (c_int, [c_void_p, c_int, c_int, P_BF, c_void_p, c_void_p, c_void_p,
                              c_void_p, c_size_t, c_void_p]),
@@ -97,6 +106,27 @@ def check(rc: int, what: str) -> None:
     if rc != NH_OK:
         msg = load().nh_last_error()
         raise NativeLibraryError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+
+KERNEL_IDS = {
+    "cnn": 0, "pfaffian": 1, "pairing": 2, "combine": 3, "hop_count": 4, "scan": 5,
+    "hop_emit": 6, "eloc_reduce": 7, "mh_propose": 8, "compact": 9, "mh_accept": 10,
+    "wtilde": 11, "pfaffian64": 12, "cnn64": 13, "flagged": 14, "pack": 15,
+}
+K_COUNT = 16
+
+
+def profile_enable(on: bool) -> None:
+    check(load().nh_profile_enable(1 if on else 0), "nh_profile_enable")
+
+
+def profile_read() -> dict:
+    """{kernel name: (milliseconds, launches)} accumulated since the last read."""
+    ms = (ctypes.c_double * K_COUNT)()
+    n = (ctypes.c_int64 * K_COUNT)()
+    check(load().nh_profile_read(ctypes.addressof(ms), ctypes.addressof(n), K_COUNT),
+          "nh_profile_read")
+    return {k: (float(ms[i]), int(n[i])) for k, i in KERNEL_IDS.items() if n[i]}
 
 
 def call(name: str, *args):

@@ -88,15 +88,17 @@ def init_params(Lx: int, Ly: int, channels: int = 32, layers: int = 4, std: floa
     return dict(conv_w=conv_w, conv_b=conv_b, W=W, theta=np.float32(0.55), Lx=Lx, Ly=Ly)
 
 
-def build_wtilde(W: torch.Tensor, theta: float, geom: PairGeometry) -> torch.Tensor:
-    """(3, N, d) -> (4, N, d) spin-block table with the distance envelope."""
+def build_wtilde(W: torch.Tensor, theta: float, geom: PairGeometry, fp64: bool = False):
+    """(3, N, d) -> (4, N, d) spin-block table with the distance envelope (FP32), and with
+    ``fp64`` also the same table in FP64: returns ``(Wt, Wt64)`` then."""
     W = _require_cuda(W, torch.float32, "W")
     if tuple(W.shape) != (3, geom.N, geom.d):
         raise ValueError(f"W shape {tuple(W.shape)} != (3, {geom.N}, {geom.d})")
     Wt = torch.empty((4, geom.N, geom.d), dtype=torch.float32, device=W.device)
+    Wt64 = torch.empty((4, geom.N, geom.d), dtype=torch.float64, device=W.device) if fp64 else None
     _lib.call("nh_build_wtilde", W.data_ptr(), float(theta), geom.LX, geom.LY, geom.d,
-              Wt.data_ptr(), stream_ptr(W.device))
-    return Wt
+              Wt.data_ptr(), _ptr(Wt64), stream_ptr(W.device))
+    return (Wt, Wt64) if fp64 else Wt
 
 
 def pairing_occ(Y: torch.Tensor, idx: torch.Tensor, Wt: torch.Tensor, geom: PairGeometry) -> torch.Tensor:
@@ -115,9 +117,14 @@ def pairing_occ(Y: torch.Tensor, idx: torch.Tensor, Wt: torch.Tensor, geom: Pair
     return F
 
 
-def slogpf(F: torch.Tensor):
+DEFAULT_COND_TAU = 100.0
+
+
+def slogpf(F: torch.Tensor, cond_tau: float = DEFAULT_COND_TAU):
     """(sign FP32, logabs FP64, flags int32) of the Pfaffians of antisymmetric F (..., n, n)
-    in FP32; only the strict lower triangle is read."""
+    in FP32; only the strict lower triangle is read.  Matrices whose pivot ratio exceeds
+    ``cond_tau`` are factorised again in FP64 (flags NH_FLAG_GROWTH | NH_FLAG_REFINED);
+    ``cond_tau=0`` keeps the plain FP32 result."""
     F = _require_cuda(F, torch.float32, "F")
     n = F.shape[-1]
     if F.shape[-2] != n:
@@ -127,8 +134,11 @@ def slogpf(F: torch.Tensor):
     sign = torch.empty(batch, dtype=torch.float32, device=F.device)
     logabs = torch.empty(batch, dtype=torch.float64, device=F.device)
     flags = torch.empty(batch, dtype=torch.int32, device=F.device)
-    _lib.call("nh_slogpf", F.data_ptr(), n, batch, sign.data_ptr(), logabs.data_ptr(),
-              flags.data_ptr(), stream_ptr(F.device))
+    nbytes = _lib.load().nh_slogpf_workspace_bytes(batch)
+    ws = workspace(nbytes, F.device, "slogpf")
+    _lib.call("nh_slogpf", F.data_ptr(), n, batch, float(cond_tau), sign.data_ptr(),
+              logabs.data_ptr(), flags.data_ptr(), ws.data_ptr(), ws.numel(),
+              stream_ptr(F.device))
     return sign.reshape(batch_shape), logabs.reshape(batch_shape), flags.reshape(batch_shape)
 
 
@@ -137,8 +147,12 @@ class PfaffianBackflow:
     backflow CNN of the graded configurations; parameters live on the GPU in FP32."""
 
     def __init__(self, Lx: int, Ly: int, n_up: int, n_dn: int, params: Optional[dict] = None,
-                 channels: int = 32, layers: int = 4, seed: int = 0, device="cuda"):
+                 channels: int = 32, layers: int = 4, seed: int = 0, device="cuda",
+                 cond_tau: float = DEFAULT_COND_TAU):
+        """``cond_tau``: items whose pivot ratio exceeds it are recomputed end to end in FP64
+        (``0`` keeps every item on the FP32 path)."""
         self.device = torch.device(device)
+        self.cond_tau = float(cond_tau)
         if params is None:
             params = init_params(Lx, Ly, channels, layers, seed=seed)
         self.channels = int(params["conv_w"][0].shape[0])
@@ -153,16 +167,20 @@ class PfaffianBackflow:
             [np.asarray(w, np.float32).ravel() for w in params["conv_w"]])).to(dev)
         self.conv_b = torch.from_numpy(np.concatenate(
             [np.asarray(b, np.float32).ravel() for b in params["conv_b"]])).to(dev)
+        self.conv_w_packed = torch.empty_like(self.conv_w)
+        _lib.call("nh_pack_cnn_weights", self.conv_w.data_ptr(), self.channels, self.layers,
+                  self.conv_w_packed.data_ptr(), stream_ptr(dev))
         self.W = torch.from_numpy(np.asarray(params["W"], np.float32)).to(dev).contiguous()
         self.theta = float(params["theta"])
-        self.Wt = build_wtilde(self.W, self.theta, self.geom)
+        self.Wt, self.Wt64 = build_wtilde(self.W, self.theta, self.geom, fp64=True)
         self.host_params = params
 
     def c_params(self) -> _lib.BackflowParams:
         g = self.geom
         return _lib.BackflowParams(self.conv_w.data_ptr(), self.conv_b.data_ptr(),
-                                   self.Wt.data_ptr(), g.LX, g.LY, g.n_up, g.n_dn, self.channels,
-                                   self.layers)
+                                   self.conv_w_packed.data_ptr(), self.Wt.data_ptr(),
+                                   self.Wt64.data_ptr(), g.LX, g.LY, g.n_up, g.n_dn,
+                                   self.channels, self.layers, self.cond_tau)
 
     def features(self, spins: torch.Tensor) -> torch.Tensor:
         """(B, 2, N, d) backflow features of int8 configurations (B, 2N)."""

@@ -4,9 +4,52 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <mutex>
+#include <vector>
+
 #include "nh_common.cuh"
 
 namespace nh {
+
+// ------------------------------------------------------------------ per-kernel timing
+namespace {
+struct ProfRecord {
+  int id;
+  cudaEvent_t a, b;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRecord> g_prof_pending;
+std::vector<cudaEvent_t> g_prof_free;
+double g_prof_ms[NH_K_COUNT];
+int64_t g_prof_n[NH_K_COUNT];
+
+cudaEvent_t prof_event() {
+  if (!g_prof_free.empty()) {
+    cudaEvent_t e = g_prof_free.back();
+    g_prof_free.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+}  // namespace
+
+ProfScope::ProfScope(int id, cudaStream_t st) : id_(id), st_(st) {
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  if (!g_prof_on) return;
+  a_ = prof_event();
+  cudaEventRecord(a_, st_);
+}
+
+ProfScope::~ProfScope() {
+  if (!a_) return;
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  cudaEvent_t b = prof_event();
+  cudaEventRecord(b, st_);
+  g_prof_pending.push_back(ProfRecord{id_, a_, b});
+}
 
 static thread_local char g_err[1024] = "";
 
@@ -43,49 +86,66 @@ int num_sms() {
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 size_t pipeline_bytes(int max_items, int n, int d) {
-  size_t it = (size_t)(max_items > 0 ? max_items : 1);
+  const size_t it = (size_t)(max_items > 0 ? max_items : 1);
   return align256(it * n * d * sizeof(float)) + align256(it * n * sizeof(int32_t)) +
          align256(it * sizeof(float)) * 2 + align256(it * sizeof(double)) +
-         align256(it * sizeof(int32_t));
+         align256(it * sizeof(int32_t)) * 2 + align256(sizeof(int32_t)) +
+         align256(it * n * d * sizeof(double)) + align256(it * n * sizeof(int32_t));
 }
 
 PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d) {
-  size_t it = (size_t)(max_items > 0 ? max_items : 1);
+  const size_t it = (size_t)(max_items > 0 ? max_items : 1);
   char* p = static_cast<char*>(ws);
+  auto take = [&](size_t bytes) {
+    char* r = p;
+    p += align256(bytes);
+    return r;
+  };
   PipelineBuffers b;
-  b.Y = reinterpret_cast<float*>(p);
-  p += align256(it * n * d * sizeof(float));
-  b.idx = reinterpret_cast<int32_t*>(p);
-  p += align256(it * n * sizeof(int32_t));
-  b.item_sign = reinterpret_cast<float*>(p);
-  p += align256(it * sizeof(float));
-  b.pf_sign = reinterpret_cast<float*>(p);
-  p += align256(it * sizeof(float));
-  b.pf_logabs = reinterpret_cast<double*>(p);
-  p += align256(it * sizeof(double));
-  b.pf_flags = reinterpret_cast<int32_t*>(p);
+  b.Y = reinterpret_cast<float*>(take(it * n * d * sizeof(float)));
+  b.idx = reinterpret_cast<int32_t*>(take(it * n * sizeof(int32_t)));
+  b.item_sign = reinterpret_cast<float*>(take(it * sizeof(float)));
+  b.pf_sign = reinterpret_cast<float*>(take(it * sizeof(float)));
+  b.pf_logabs = reinterpret_cast<double*>(take(it * sizeof(double)));
+  b.pf_flags = reinterpret_cast<int32_t*>(take(it * sizeof(int32_t)));
+  b.list = reinterpret_cast<int32_t*>(take(it * sizeof(int32_t)));
+  b.count = reinterpret_cast<int32_t*>(take(sizeof(int32_t)));
+  b.Y64 = reinterpret_cast<double*>(take(it * n * d * sizeof(double)));
+  b.idx64 = reinterpret_cast<int32_t*>(take(it * n * sizeof(int32_t)));
   return b;
 }
 
+// CNN -> gather + Pfaffian (FP32) -> FP64 recompute of the items flagged ill-conditioned ->
+// combination of the symmetry images (or a copy for G = 1).
 int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const PipelineBuffers& b,
                  float* sign, double* logabs, int32_t* flags, cudaStream_t st) {
   const int n = p.n_up + p.n_dn, d = p.channels / 2;
   const int max_items = cl.n_cfg * cl.G;
   if (max_items <= 0) return NH_OK;
-  int rc = launch_cnn(cl, p, 1, nullptr, b.Y, b.idx, b.item_sign, st);
+  CnnLaunch c{&cl, &p, 1, false, nullptr, nullptr, 0, nullptr, b.Y, b.idx, b.item_sign};
+  int rc = launch_cnn(c, st);
   if (rc) return rc;
-  if (cl.G == 1)
-    return launch_pfaffian_gather(b.Y, b.idx, p.Wt, p.Lx, p.Ly, d, n, max_items, &cl,
-                                  b.item_sign, sign, logabs, flags, st);
-  rc = launch_pfaffian_gather(b.Y, b.idx, p.Wt, p.Lx, p.Ly, d, n, max_items, &cl, b.item_sign,
-                              b.pf_sign, b.pf_logabs, b.pf_flags, st);
-  if (rc) return rc;
+  PfGatherArgs g{b.Y, b.idx, p.Wt, p.Lx, p.Ly, d, n, cl.n_cfg_dev, cl.G, max_items, nullptr,
+                 b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, p.cond_tau, 0, false};
+  if ((rc = launch_pfaffian_gather(g, st))) return rc;
+  if (p.Wt64 && p.cond_tau > 0.0 && pfaffian64_fits(n) && cnn64_fits(p.Lx * p.Ly, p.channels)) {
+    if ((rc = launch_flagged(b.pf_flags, max_items, cl.n_cfg_dev, cl.G, b.list, b.count, st)))
+      return rc;
+    CnnLaunch c64{&cl, &p, 1, true, b.list, b.count, max_items, nullptr, b.Y64, b.idx64,
+                  b.item_sign};
+    if ((rc = launch_cnn(c64, st))) return rc;
+    PfGatherArgs g64{b.Y64, b.idx64, p.Wt64, p.Lx, p.Ly, d, n, b.count, 1, max_items, b.list,
+                     b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, 0.0,
+                     NH_FLAG_GROWTH | NH_FLAG_REFINED, true};
+    if ((rc = launch_pfaffian_gather(g64, st))) return rc;
+  }
   return launch_combine(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev, sign,
                         logabs, flags, st);
 }
 
 static int check_params(const nh_backflow_params* p) {
-  if (!p || !p->conv_w || !p->conv_b || !p->Wt) return fail(NH_ERR_INVALID, "null parameter pointer");
+  if (!p || !p->conv_w || !p->conv_b || !p->Wt || !p->conv_w_packed)
+    return fail(NH_ERR_INVALID, "null parameter pointer (conv_w, conv_b, conv_w_packed, Wt)");
   if (p->Lx < 3 || p->Ly < 3 || p->Lx * p->Ly > kMaxN)
     return fail(NH_ERR_UNSUPPORTED, "lattice %dx%d (3 <= L, N <= %d)", p->Lx, p->Ly, kMaxN);
   const int n = p->n_up + p->n_dn;
@@ -107,24 +167,66 @@ extern "C" {
 
 int nh_abi_version(void) { return NH_ABI_VERSION; }
 
+int nh_profile_enable(int on) {
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  g_prof_on = on != 0;
+  return NH_OK;
+}
+
+int nh_profile_read(double* ms, int64_t* launches, int n_ids) {
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  int rc = NH_OK;
+  for (const ProfRecord& r : g_prof_pending) {
+    float t = 0.0f;
+    cudaError_t e = cudaEventSynchronize(r.b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, r.a, r.b);
+    if (e != cudaSuccess && rc == NH_OK) rc = check_cuda(e, "profile_read");
+    if (r.id >= 0 && r.id < NH_K_COUNT) {
+      g_prof_ms[r.id] += t;
+      g_prof_n[r.id] += 1;
+    }
+    g_prof_free.push_back(r.a);
+    g_prof_free.push_back(r.b);
+  }
+  g_prof_pending.clear();
+  for (int i = 0; i < n_ids && i < NH_K_COUNT; ++i) {
+    if (ms) ms[i] = g_prof_ms[i];
+    if (launches) launches[i] = g_prof_n[i];
+  }
+  for (int i = 0; i < NH_K_COUNT; ++i) {
+    g_prof_ms[i] = 0.0;
+    g_prof_n[i] = 0;
+  }
+  return rc;
+}
+
 const char* nh_last_error(void) { return g_err; }
 
-int nh_build_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, void* stream) {
+int nh_build_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, double* Wt64,
+                    void* stream) {
   if (!W || !Wt) return fail(NH_ERR_INVALID, "build_wtilde: null pointer");
   if (Lx < 1 || Ly < 1 || Lx * Ly > kMaxN || d < 1)
     return fail(NH_ERR_UNSUPPORTED, "build_wtilde: %dx%d, d=%d", Lx, Ly, d);
-  return launch_wtilde(W, theta, Lx, Ly, d, Wt, static_cast<cudaStream_t>(stream));
+  return launch_wtilde(W, theta, Lx, Ly, d, Wt, Wt64, static_cast<cudaStream_t>(stream));
+}
+
+int nh_pack_cnn_weights(const float* conv_w, int channels, int layers, float* packed,
+                        void* stream) {
+  if (!conv_w || !packed || channels < 1 || layers < 1)
+    return fail(NH_ERR_INVALID, "pack_cnn_weights: bad arguments");
+  return launch_pack_cnn(conv_w, channels, layers, packed, static_cast<cudaStream_t>(stream));
 }
 
 int nh_cnn_forward(const int8_t* spins, int batch, const nh_backflow_params* p, float* features,
                    void* stream) {
-  if (!p || !p->conv_w || !p->conv_b) return fail(NH_ERR_INVALID, "cnn_forward: null parameters");
+  if (!p || !p->conv_w_packed || !p->conv_b)
+    return fail(NH_ERR_INVALID, "cnn_forward: null parameters");
   if (!spins || !features || batch < 0) return fail(NH_ERR_INVALID, "cnn_forward: bad buffers");
   if (p->Lx < 3 || p->Ly < 3 || p->Lx * p->Ly > kMaxN)
     return fail(NH_ERR_UNSUPPORTED, "cnn_forward: lattice %dx%d", p->Lx, p->Ly);
   ConfigList cl{spins, nullptr, nullptr, nullptr, nullptr, batch, 1};
-  return launch_cnn(cl, *p, 0, features, nullptr, nullptr, nullptr,
-                    static_cast<cudaStream_t>(stream));
+  CnnLaunch c{&cl, p, 0, false, nullptr, nullptr, 0, features, nullptr, nullptr, nullptr};
+  return launch_cnn(c, static_cast<cudaStream_t>(stream));
 }
 
 int nh_pairing_occ(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
@@ -136,12 +238,28 @@ int nh_pairing_occ(const float* Y, const int32_t* idx, const float* Wt, int Lx, 
   return launch_pairing(Y, idx, Wt, Lx, Ly, d, n, batch, F, static_cast<cudaStream_t>(stream));
 }
 
-int nh_slogpf(const float* F, int n, int batch, float* sign, double* logabs, int32_t* flags,
-              void* stream) {
+size_t nh_slogpf_workspace_bytes(int batch) {
+  return align256((size_t)(batch > 0 ? batch : 1) * sizeof(int32_t)) + align256(sizeof(int32_t));
+}
+
+int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, double* logabs,
+              int32_t* flags, void* workspace, size_t workspace_bytes, void* stream) {
   if (!F || !sign || !logabs || batch < 0) return fail(NH_ERR_INVALID, "slogpf: bad arguments");
   if (batch == 0) return NH_OK;
-  return launch_pfaffian_from_F(F, n, batch, sign, logabs, flags,
-                                static_cast<cudaStream_t>(stream));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const bool refine = cond_tau > 0.0;
+  if (refine && (!flags || !workspace || workspace_bytes < nh_slogpf_workspace_bytes(batch)))
+    return fail(NH_ERR_WORKSPACE, "slogpf: refinement needs flags and %zu B of workspace",
+                nh_slogpf_workspace_bytes(batch));
+  int rc = launch_pfaffian_from_F(F, n, batch, nullptr, nullptr, false, cond_tau, 0, sign,
+                                  logabs, flags, st);
+  if (rc || !refine || !pfaffian64_fits(n)) return rc;  // too large for FP64: flags only
+  int32_t* list = static_cast<int32_t*>(workspace);
+  int32_t* count = reinterpret_cast<int32_t*>(static_cast<char*>(workspace) +
+                                              align256((size_t)batch * sizeof(int32_t)));
+  if ((rc = launch_flagged(flags, batch, nullptr, 1, list, count, st))) return rc;
+  return launch_pfaffian_from_F(F, n, batch, list, count, true, 0.0,
+                                NH_FLAG_GROWTH | NH_FLAG_REFINED, sign, logabs, flags, st);
 }
 
 size_t nh_amplitude_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p) {
@@ -235,8 +353,9 @@ int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs
   const int N = p->Lx * p->Ly, n = p->n_up + p->n_dn, d = p->channels / 2;
   if ((rc = launch_hop_count(spins, batch, p->Lx, p->Ly, h->n_dirs, L.counts, st))) return rc;
   if ((rc = launch_scan_counts(L.counts, batch, L.offsets, st))) return rc;
-  if ((rc = launch_hop_emit(spins, batch, p->Lx, p->Ly, *h, L.offsets, nullptr, L.hval, L.owner,
-                            L.from, L.to, st)))
+  const int64_t cmax = (int64_t)batch * n * 8;
+  if ((rc = launch_hop_emit(spins, batch, p->Lx, p->Ly, *h, L.offsets, cmax, nullptr, L.hval,
+                            L.owner, L.from, L.to, st)))
     return rc;
   int64_t total = 0;
   if ((rc = check_cuda(cudaMemcpyAsync(&total, L.offsets + batch, sizeof(int64_t),
@@ -245,6 +364,9 @@ int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs
     return rc;
   if ((rc = check_cuda(cudaStreamSynchronize(st), "local_energy: sync"))) return rc;
   if (n_conn_out) *n_conn_out = total;
+  if (total > cmax)
+    return fail(NH_ERR_INVALID, "local_energy: %lld connections exceed %lld (more than %d "
+                "electrons in a configuration)", (long long)total, (long long)cmax, n);
   PipelineBuffers b = carve_pipeline(L.pipe, chunk * n_symm, n, d);
   for (int64_t c0 = 0; c0 < total; c0 += chunk) {
     const int nc = (int)((total - c0) < chunk ? (total - c0) : chunk);
@@ -267,8 +389,9 @@ int nh_hop_list(const int8_t* spins, int batch, int Lx, int Ly, const nh_hubbard
   if ((rc = launch_hop_count(spins, batch, Lx, Ly, h->n_dirs, counts, st))) return rc;
   if ((rc = launch_scan_counts(counts, batch, offsets, st))) return rc;
   if (!rec && !hval) return NH_OK;
-  return launch_hop_emit(spins, batch, Lx, Ly, *h, offsets, rec, hval, nullptr, nullptr, nullptr,
-                         st);
+  // rec / hval must hold batch * (electrons per configuration) * n_dirs records.
+  return launch_hop_emit(spins, batch, Lx, Ly, *h, offsets, INT64_MAX, rec, hval, nullptr,
+                         nullptr, nullptr, st);
 }
 
 // ------------------------------------------------------------------ Metropolis sampler

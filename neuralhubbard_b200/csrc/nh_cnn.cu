@@ -1,9 +1,11 @@
-// Backflow CNN forward, FP32 on CUDA cores (the plain form).
+// Backflow CNN forward on CUDA cores, FP32 (the plain form) or FP64 (recompute of items flagged
+// ill-conditioned), and the weight packing it reads.
 //
 // One CTA per item (configuration x symmetry image, grid-stride).  The item's configuration
 // is built in shared memory from the int8 sample, its optional hop and the image map, then the
-// 4 periodic 3x3 layers run with both activation buffers resident in shared memory
-// (channel-major, row stride N + 1).  Output mode 0 writes the features (2, N, d) of
+// periodic 3x3 layers run with both activation buffers resident in shared memory
+// (channel-major, row stride N + 1) and each layer's weights staged there in the packed
+// [ci][tap][co] layout.  Output mode 0 writes the features (2, N, d) of
 // code/backflow/models.py:163-167; mode 1 writes only the occupied rows Y (n, d) of the image
 // configuration in ascending mode order (the gather y.reshape(2N, d)[idx] of
 // code/backflow/pf_kernel.py:395), the occupied mode list idx (n,) and the item sign
@@ -16,14 +18,18 @@
 namespace nh {
 namespace {
 
+template <typename T>
 struct CnnArgs {
   ConfigList cl;
-  const float* w;
+  const float* wp;  // packed weights, per layer [ci][tap][co]
   const float* b;
   int Lx, Ly, N, C, layers, n;
   int mode;
+  const int32_t* slot_item;   // slot -> item, null: identity over all items
+  const int32_t* slot_count;  // device number of slots when slot_item is set
+  int max_slots;
   float* feat;
-  float* Y;
+  T* Y;
   int32_t* idx;
   float* item_sign;
 };
@@ -31,6 +37,27 @@ struct CnnArgs {
 __device__ __forceinline__ float gelu_tanh(float x) {
   const float k0 = 0.7978845608028654f;  // sqrt(2 / pi)
   return 0.5f * x * (1.0f + tanhf(k0 * (x + 0.044715f * x * x * x)));
+}
+__device__ __forceinline__ double gelu_tanh(double x) {
+  const double k0 = 0.7978845608028654;
+  return 0.5 * x * (1.0 + tanh(k0 * (x + 0.044715 * x * x * x)));
+}
+__device__ __forceinline__ float tfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double tfma(double a, double b, double c) { return fma(a, b, c); }
+
+__device__ __forceinline__ void lds8(const float* p, float* o) {
+  const float4 a = reinterpret_cast<const float4*>(p)[0];
+  const float4 b = reinterpret_cast<const float4*>(p)[1];
+  o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+  o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+}
+__device__ __forceinline__ void lds8(const double* p, double* o) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double2 v = reinterpret_cast<const double2*>(p)[k];
+    o[2 * k] = v.x;
+    o[2 * k + 1] = v.y;
+  }
 }
 
 // Exclusive block scan of one int per thread; returns the exclusive prefix, *total the sum.
@@ -60,25 +87,27 @@ __device__ __forceinline__ int block_scan(int v, int* warp_buf, int* total) {
   return base + x - v;
 }
 
-__global__ void __launch_bounds__(kNumThreads) cnn_fp32_kernel(CnnArgs a) {
+template <typename T>
+__global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = a.N, C = a.C, NS = N + 1, M2 = 2 * N;
   const int tid = threadIdx.x;
-  float* actA = reinterpret_cast<float*>(smem_raw);
-  float* actB = actA + C * NS;
-  float* wsm = actB + C * NS;      // [ci][tap][co]
-  float* bsm = wsm + C * C * 9;    // [co]
+  T* actA = reinterpret_cast<T*>(smem_raw);
+  T* actB = actA + C * NS;
+  T* wsm = actB + C * NS;      // [ci][tap][co]
+  T* bsm = wsm + C * C * 9;    // [co]
   int* simg = reinterpret_cast<int*>(bsm + C);  // (2N) +-1 of the image configuration
-  int* occl = simg + M2;           // (2N) ascending occupied modes of the image configuration
-  int* wbuf = occl + M2;           // 32 ints of scan scratch
+  int* occl = simg + M2;       // (2N) ascending occupied modes of the image configuration
+  int* wbuf = occl + M2;       // 32 ints of scan scratch
 
-  const int n_cfg = a.cl.n_cfg_dev ? *a.cl.n_cfg_dev : a.cl.n_cfg;
   const int G = a.cl.G;
-  const int n_items = n_cfg * G;
+  const int n_work = a.slot_item ? *a.slot_count
+                                 : (a.cl.n_cfg_dev ? *a.cl.n_cfg_dev : a.cl.n_cfg) * G;
   const int half = N / 2;
   const int ngroups = C / 8;
 
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+  for (int slot = blockIdx.x; slot < n_work; slot += gridDim.x) {
+    const int item = a.slot_item ? a.slot_item[slot] : slot;
     const int c = item / G, g = item - c * G;
     const int smp = a.cl.sample ? a.cl.sample[c] : c;
     const int fr = a.cl.from ? a.cl.from[c] : -1;
@@ -87,27 +116,23 @@ __global__ void __launch_bounds__(kNumThreads) cnn_fp32_kernel(CnnArgs a) {
 
     __syncthreads();  // previous item's readers of simg/act are done
     for (int m = tid; m < M2; m += kNumThreads) {
-      int src = sym_map(m, g, a.Lx, a.Ly, N);  // image[m] = s[g(m)] (g is an involution)
+      const int src = sym_map(m, g, a.Lx, a.Ly, N);  // image[m] = s[g(m)] (g is an involution)
       int v = base[src];
       v = (src == fr) ? -1 : ((src == to) ? 1 : v);
       simg[m] = v > 0 ? 1 : -1;
-      int ch = m >= N ? 1 : 0;
-      actA[ch * NS + (m - ch * N)] = v > 0 ? 1.0f : -1.0f;
+      const int ch = m >= N ? 1 : 0;
+      actA[ch * NS + (m - ch * N)] = v > 0 ? T(1) : T(-1);
     }
 
-    float* in = actA;
-    float* out = actB;
+    T* in = actA;
+    T* out = actB;
     int cin = 2;
-    const float* wl = a.w;
+    const float* wl = a.wp;
     for (int l = 0; l < a.layers; ++l) {
       __syncthreads();
       const int cnt = C * cin * 9;
-      for (int i = tid; i < cnt; i += kNumThreads) {
-        int co = i / (cin * 9);
-        int rem = i - co * cin * 9;  // ci * 9 + tap
-        wsm[rem * C + co] = wl[i];
-      }
-      for (int i = tid; i < C; i += kNumThreads) bsm[i] = a.b[l * C + i];
+      for (int i = tid; i < cnt; i += kNumThreads) wsm[i] = T(__ldg(wl + i));
+      for (int i = tid; i < C; i += kNumThreads) bsm[i] = T(__ldg(a.b + l * C + i));
       __syncthreads();
       const bool act_fn = l < a.layers - 1;
       for (int task = tid; task < ngroups * half; task += kNumThreads) {
@@ -115,11 +140,11 @@ __global__ void __launch_bounds__(kNumThreads) cnn_fp32_kernel(CnnArgs a) {
         const int s0 = task - grp * half, s1 = s0 + half;
         const int x0 = s0 / a.Ly, y0 = s0 - x0 * a.Ly;
         const int x1 = s1 / a.Ly, y1 = s1 - x1 * a.Ly;
-        float acc0[8], acc1[8];
+        T acc0[8], acc1[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) acc0[j] = acc1[j] = bsm[grp * 8 + j];
         for (int ci = 0; ci < cin; ++ci) {
-          const float* inc = in + ci * NS;
+          const T* inc = in + ci * NS;
 #pragma unroll
           for (int u = 0; u < 3; ++u) {
             int xa = x0 + u - 1, xb = x1 + u - 1;
@@ -130,31 +155,27 @@ __global__ void __launch_bounds__(kNumThreads) cnn_fp32_kernel(CnnArgs a) {
               int ya = y0 + v - 1, yb = y1 + v - 1;
               ya = ya < 0 ? ya + a.Ly : (ya >= a.Ly ? ya - a.Ly : ya);
               yb = yb < 0 ? yb + a.Ly : (yb >= a.Ly ? yb - a.Ly : yb);
-              const float i0 = inc[xa * a.Ly + ya];
-              const float i1 = inc[xb * a.Ly + yb];
-              const float4* wp =
-                  reinterpret_cast<const float4*>(wsm + (ci * 9 + u * 3 + v) * C + grp * 8);
-              const float4 wa = wp[0], wb = wp[1];
-              const float w8[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+              const T i0 = inc[xa * a.Ly + ya];
+              const T i1 = inc[xb * a.Ly + yb];
+              T w8[8];
+              lds8(wsm + (ci * 9 + u * 3 + v) * C + grp * 8, w8);
 #pragma unroll
               for (int j = 0; j < 8; ++j) {
-                acc0[j] = fmaf(i0, w8[j], acc0[j]);
-                acc1[j] = fmaf(i1, w8[j], acc1[j]);
+                acc0[j] = tfma(i0, w8[j], acc0[j]);
+                acc1[j] = tfma(i1, w8[j], acc1[j]);
               }
             }
           }
         }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          float r0 = act_fn ? gelu_tanh(acc0[j]) : acc0[j];
-          float r1 = act_fn ? gelu_tanh(acc1[j]) : acc1[j];
-          out[(grp * 8 + j) * NS + s0] = r0;
-          out[(grp * 8 + j) * NS + s1] = r1;
+          out[(grp * 8 + j) * NS + s0] = act_fn ? gelu_tanh(acc0[j]) : acc0[j];
+          out[(grp * 8 + j) * NS + s1] = act_fn ? gelu_tanh(acc1[j]) : acc1[j];
         }
       }
       wl += C * cin * 9;
       cin = C;
-      float* t = in;
+      T* t = in;
       in = out;
       out = t;
     }
@@ -163,10 +184,10 @@ __global__ void __launch_bounds__(kNumThreads) cnn_fp32_kernel(CnnArgs a) {
     if (a.mode == 0) {
       float* dst = a.feat + (int64_t)item * C * N;
       for (int o = tid; o < C * N; o += kNumThreads) {
-        int aa = o % d;
-        int site = (o / d) % N;
-        int sg = o / (N * d);
-        dst[o] = in[(sg * d + aa) * NS + site];
+        const int aa = o % d;
+        const int site = (o / d) % N;
+        const int sg = o / (N * d);
+        dst[o] = (float)in[(sg * d + aa) * NS + site];
       }
       continue;
     }
@@ -181,29 +202,29 @@ __global__ void __launch_bounds__(kNumThreads) cnn_fp32_kernel(CnnArgs a) {
       if (simg[m] > 0) occl[pos++] = m;
     __syncthreads();
     const int n = a.n;
-    float* Ydst = a.Y + (int64_t)item * n * d;
+    T* Ydst = a.Y + (int64_t)slot * n * d;
     for (int o = tid; o < n * d; o += kNumThreads) {
-      int p = o / d, aa = o - p * d;
-      int m = occl[p < total ? p : 0];
-      int sg = m >= N ? 1 : 0;
+      const int p = o / d, aa = o - p * d;
+      const int m = occl[p < total ? p : 0];
+      const int sg = m >= N ? 1 : 0;
       Ydst[o] = in[(sg * d + aa) * NS + (m - sg * N)];
     }
-    int32_t* idst = a.idx + (int64_t)item * n;
+    int32_t* idst = a.idx + (int64_t)slot * n;
     for (int p = tid; p < n; p += kNumThreads) idst[p] = occl[p < total ? p : 0];
     // eta_g: parity of the inversions of (g(a_1), ..., g(a_n)).
     int par = 0;
     if (g != 0) {
       for (int i = tid; i < total; i += kNumThreads) {
-        int gi = sym_map(occl[i], g, a.Lx, a.Ly, N);
+        const int gi = sym_map(occl[i], g, a.Lx, a.Ly, N);
         int inv = 0;
         for (int j = i + 1; j < total; ++j) inv += sym_map(occl[j], g, a.Lx, a.Ly, N) < gi;
         par ^= inv & 1;
       }
     }
-    int odd = __syncthreads_count(par);
+    const int odd = __syncthreads_count(par);
     if (tid == 0) {
-      long long kk = total;
-      int rev = (int)((kk * (kk - 1) / 2) & 1);
+      const long long kk = total;
+      const int rev = (int)((kk * (kk - 1) / 2) & 1);
       float s = ((odd & 1) ^ rev) ? -1.0f : 1.0f;
       if (total != n) s = 0.0f;  // wrong particle number: amplitude 0
       a.item_sign[item] = s;
@@ -211,48 +232,85 @@ __global__ void __launch_bounds__(kNumThreads) cnn_fp32_kernel(CnnArgs a) {
   }
 }
 
+// packed[l][ci][tap][co] = conv_w[l][co][ci][tap]
+__global__ void pack_kernel(const float* __restrict__ w, int C, int layers, float* packed) {
+  const int total = 18 * C + (layers - 1) * 9 * C * C;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    int l = 0, off = 0, cin = 2;
+    if (i >= 18 * C) {
+      l = 1 + (i - 18 * C) / (9 * C * C);
+      off = 18 * C + (l - 1) * 9 * C * C;
+      cin = C;
+    }
+    const int r = i - off;  // (ci * 9 + tap) * C + co
+    const int co = r % C;
+    const int ct = r / C;  // ci * 9 + tap
+    packed[i] = w[off + co * cin * 9 + ct];
+  }
+}
+
+template <typename T>
+size_t cnn_smem(int N, int C) {
+  return sizeof(T) * (2 * (size_t)C * (N + 1) + (size_t)C * C * 9 + C) +
+         sizeof(int) * (4 * (size_t)N + 32);
+}
+
 }  // namespace
 
-int launch_cnn(const ConfigList& cl, const nh_backflow_params& p, int out_mode, float* feat,
-               float* Y, int32_t* idx, float* item_sign, cudaStream_t st) {
-  CnnArgs a;
-  a.cl = cl;
-  a.w = p.conv_w;
-  a.b = p.conv_b;
-  a.Lx = p.Lx;
-  a.Ly = p.Ly;
-  a.N = p.Lx * p.Ly;
-  a.C = p.channels;
-  a.layers = p.layers;
-  a.n = p.n_up + p.n_dn;
-  a.mode = out_mode;
-  a.feat = feat;
-  a.Y = Y;
-  a.idx = idx;
-  a.item_sign = item_sign;
-  if (a.C % 16 || a.C < 16 || a.C > 64 || a.layers < 1 || a.N % 2 || a.N > kMaxN)
+bool cnn64_fits(int N, int C) { return cnn_smem<double>(N, C) <= 227 * 1024; }
+
+int launch_pack_cnn(const float* conv_w, int channels, int layers, float* packed, cudaStream_t st) {
+  const int total = 18 * channels + (layers - 1) * 9 * channels * channels;
+  ProfScope prof_scope(NH_K_PACK, st);
+  pack_kernel<<<(total + 255) / 256, 256, 0, st>>>(conv_w, channels, layers, packed);
+  return check_launch("pack_kernel");
+}
+
+int launch_cnn(const CnnLaunch& q, cudaStream_t st) {
+  const nh_backflow_params& p = *q.p;
+  const int N = p.Lx * p.Ly, C = p.channels;
+  if (C % 16 || C < 16 || C > 64 || p.layers < 1 || N % 2 || N > kMaxN)
     return fail(NH_ERR_UNSUPPORTED, "cnn: channels %d (multiple of 16, <= 64), layers %d, N %d",
-                a.C, a.layers, a.N);
-  const int N = a.N, C = a.C;
-  size_t smem = sizeof(float) * (2 * (size_t)C * (N + 1) + (size_t)C * C * 9 + C) +
-                sizeof(int) * (4 * (size_t)N + 32);
+                C, p.layers, N);
+  if (!p.conv_w_packed)
+    return fail(NH_ERR_INVALID, "cnn: conv_w_packed is null (call nh_pack_cnn_weights)");
+  const size_t smem = q.fp64 ? cnn_smem<double>(N, C) : cnn_smem<float>(N, C);
   if (smem > 227 * 1024)
-    return fail(NH_ERR_UNSUPPORTED, "cnn: lattice N=%d with %d channels needs %zu B of smem", N,
-                C, smem);
+    return fail(NH_ERR_UNSUPPORTED, "cnn: lattice N=%d with %d channels needs %zu B of smem "
+                "(%s)", N, C, smem, q.fp64 ? "FP64" : "FP32");
+  const int slots = q.slot_item ? q.max_slots : q.cl->n_cfg * q.cl->G;
+  if (slots <= 0) return NH_OK;
+  const int per_sm = smem > 113 * 1024 ? 1 : 2;
+  int grid = num_sms() * per_sm * 4;
+  if (grid > slots) grid = slots;
+  if (q.fp64) {
+    static size_t configured = 0;
+    if (smem > 48 * 1024 && smem > configured) {
+      cudaError_t e = cudaFuncSetAttribute(cnn_kernel<double>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return check_cuda(e, "cnn smem attribute");
+      configured = smem;
+    }
+    CnnArgs<double> a{*q.cl, p.conv_w_packed, p.conv_b, p.Lx, p.Ly, N, C, p.layers,
+                      p.n_up + p.n_dn, q.mode, q.slot_item, q.slot_count, q.max_slots,
+                      q.feat, static_cast<double*>(q.Y), q.idx, q.item_sign};
+    ProfScope prof_scope(NH_K_CNN64, st);
+    cnn_kernel<double><<<grid, kNumThreads, smem, st>>>(a);
+    return check_launch("cnn_kernel<double>");
+  }
   static size_t configured = 0;
   if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(cnn_fp32_kernel,
+    cudaError_t e = cudaFuncSetAttribute(cnn_kernel<float>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return check_cuda(e, "cnn smem attribute");
     configured = smem;
   }
-  int items = cl.n_cfg * cl.G;
-  if (items <= 0) return NH_OK;
-  int per_sm = smem > 113 * 1024 ? 1 : 2;
-  int grid = num_sms() * per_sm * 4;
-  if (grid > items) grid = items;
-  cnn_fp32_kernel<<<grid, kNumThreads, smem, st>>>(a);
-  return check_launch("cnn_fp32_kernel");
+  CnnArgs<float> a{*q.cl, p.conv_w_packed, p.conv_b, p.Lx, p.Ly, N, C, p.layers,
+                   p.n_up + p.n_dn, q.mode, q.slot_item, q.slot_count, q.max_slots,
+                   q.feat, static_cast<float*>(q.Y), q.idx, q.item_sign};
+  ProfScope prof_scope(NH_K_CNN, st);
+  cnn_kernel<float><<<grid, kNumThreads, smem, st>>>(a);
+  return check_launch("cnn_kernel<float>");
 }
 
 }  // namespace nh

@@ -89,26 +89,67 @@ struct PipelineBuffers {
   float* pf_sign;     // (items,)
   double* pf_logabs;  // (items,)
   int32_t* pf_flags;  // (items,)
+  int32_t* list;      // (items,) items recomputed in FP64
+  int32_t* count;     // (1,) their number
+  double* Y64;        // (items, n, d)
+  int32_t* idx64;     // (items, n)
 };
 
 size_t pipeline_bytes(int max_items, int n, int d);
 PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d);
 
+// CNN launch: all items of a configuration list (slot = item), or the items of a device list.
+struct CnnLaunch {
+  const ConfigList* cl;
+  const nh_backflow_params* p;
+  int mode;                   // 0: features (items, 2, N, d) FP32; 1: occupied Y + idx + sign
+  bool fp64;                  // FP64 activations and outputs (mode 1 only)
+  const int32_t* slot_item;   // slot -> item, null: identity
+  const int32_t* slot_count;  // device number of slots when slot_item is set
+  int max_slots;
+  float* feat;
+  void* Y;                    // float or double (fp64)
+  int32_t* idx;
+  float* item_sign;
+};
+
+struct PfGatherArgs {
+  const void* Y;       // (slots, n, d) float or double
+  const int32_t* idx;  // (slots, n)
+  const void* Wt;      // (4, N, d) float or double
+  int Lx, Ly, d, n;
+  const int32_t* count_dev;  // device work count (times count_mult) or null
+  int count_mult;
+  int n_slots;
+  const int32_t* slot_item;  // slot -> item, null: identity
+  const float* item_sign;
+  float* sign;
+  double* logabs;
+  int32_t* flags;
+  double cond_tau;
+  int flag_or;
+  bool fp64;
+};
+
 // Launchers (return NH_OK or an error code).
-int launch_cnn(const ConfigList& cl, const nh_backflow_params& p, int out_mode, float* feat,
-               float* Y, int32_t* idx, float* item_sign, cudaStream_t st);
-int launch_pfaffian_from_F(const float* F, int n, int batch, float* sign, double* logabs,
-                           int32_t* flags, cudaStream_t st);
-int launch_pfaffian_gather(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly,
-                           int d, int n, int max_items, const ConfigList* cl,
-                           const float* item_sign, float* sign, double* logabs, int32_t* flags,
-                           cudaStream_t st);
+int launch_cnn(const CnnLaunch& q, cudaStream_t st);
+int launch_pack_cnn(const float* conv_w, int channels, int layers, float* packed, cudaStream_t st);
+int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list,
+                           const int32_t* count, bool fp64, double cond_tau, int flag_or,
+                           float* sign, double* logabs, int32_t* flags, cudaStream_t st);
+int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st);
 int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
                    int n, int batch, float* F, cudaStream_t st);
 int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, int n_cfg,
                    const int32_t* n_cfg_dev, float* sign, double* logabs, int32_t* flags,
                    cudaStream_t st);
-int launch_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, cudaStream_t st);
+int launch_flagged(const int32_t* flags, int n_items, const int32_t* count_dev, int count_mult,
+                   int32_t* list, int32_t* count, cudaStream_t st);
+int launch_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, double* Wt64,
+                  cudaStream_t st);
+// Whether the FP64 kernels fit in shared memory (n x n Pfaffian; N sites x C channels CNN).
+bool pfaffian64_fits(int n);
+bool cnn64_fits(int N, int C);
 
 // Full amplitude of a configuration list: CNN -> gather + Pfaffian -> image combination.
 int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const PipelineBuffers& b,
@@ -118,9 +159,11 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
 int launch_hop_count(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs,
                      int32_t* counts, cudaStream_t st);
 int launch_scan_counts(const int32_t* counts, int batch, int64_t* offsets, cudaStream_t st);
+// Writes at most cap records (connections beyond cap, only possible for configurations with
+// more electrons than the buffers were sized for, are dropped; callers check the total).
 int launch_hop_emit(const int8_t* spins, int batch, int Lx, int Ly, const nh_hubbard_params& h,
-                    const int64_t* offsets, int32_t* rec, double* hval, int32_t* owner,
-                    int32_t* from, int32_t* to, cudaStream_t st);
+                    const int64_t* offsets, int64_t cap, int32_t* rec, double* hval,
+                    int32_t* owner, int32_t* from, int32_t* to, cudaStream_t st);
 int launch_eloc_reduce(const int8_t* spins, const float* sign, const double* logabs, int batch,
                        int N, double U, const int64_t* offsets, const double* hval,
                        const float* csign, const double* clogabs, double* eloc,
@@ -137,5 +180,18 @@ int launch_mh_accept(int8_t* spins, float* sign, double* logabs, int batch, int 
                      uint64_t seed, int64_t step, int32_t* accepted, cudaStream_t st);
 
 int num_sms();
+
+// Per-kernel CUDA-event timing (enabled by nh_profile_enable).  Construct before the launch,
+// destroy after it: records an event pair on the launching stream when profiling is on.
+class ProfScope {
+ public:
+  ProfScope(int id, cudaStream_t st);
+  ~ProfScope();
+
+ private:
+  int id_;
+  cudaStream_t st_;
+  cudaEvent_t a_ = nullptr;
+};
 
 }  // namespace nh

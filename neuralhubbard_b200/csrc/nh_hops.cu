@@ -48,9 +48,10 @@ __global__ void __launch_bounds__(kNumThreads) hop_kernel(const int8_t* __restri
                                                           int batch, int Lx, int Ly, int n_dirs,
                                                           double t, double tp,
                                                           int32_t* counts,
-                                                          const int64_t* offsets, int32_t* rec,
-                                                          double* hval, int32_t* owner,
-                                                          int32_t* cfrom, int32_t* cto) {
+                                                          const int64_t* offsets, int64_t cap,
+                                                          int32_t* rec, double* hval,
+                                                          int32_t* owner, int32_t* cfrom,
+                                                          int32_t* cto) {
   __shared__ int occ[2 * kMaxN];
   __shared__ int pre[2 * kMaxN + 1];
   __shared__ int buf[32];
@@ -99,6 +100,7 @@ __global__ void __launch_bounds__(kNumThreads) hop_kernel(const int8_t* __restri
         const int lo = m < mj ? m : mj, hi = m < mj ? mj : m;
         const int between = pre[hi] - pre[lo + 1];
         const double amp = d < 4 ? t : tp;
+        if (o >= cap) break;  // more electrons than the buffers were sized for
         if (rec) {
           rec[2 * o] = m;
           rec[2 * o + 1] = mj;
@@ -290,7 +292,8 @@ __global__ void mh_accept_kernel(int8_t* spins, float* sign, double* logabs, int
 // Wt (4, N, d) = [uu, ud, du, dd] blocks times exp(-lam D_r) / (N sum_r exp(-lam D_r)),
 // lam = softplus(theta) (code/backflow/pf_kernel.py:107-124).  Single CTA.
 __global__ void __launch_bounds__(1024) wtilde_kernel(const float* __restrict__ W, float theta,
-                                                      int Lx, int Ly, int d, float* Wt) {
+                                                      int Lx, int Ly, int d, float* Wt,
+                                                      double* Wt64) {
   __shared__ double part[32];
   __shared__ double total;
   const int N = Lx * Ly;
@@ -319,17 +322,25 @@ __global__ void __launch_bounds__(1024) wtilde_kernel(const float* __restrict__ 
     const int rx = r / Ly, ry = r - rx * Ly;
     const int nr = (rx ? Lx - rx : 0) * Ly + (ry ? Ly - ry : 0);
     const double mx = (double)min(rx, Lx - rx), my = (double)min(ry, Ly - ry);
-    const float pref = (float)(exp(-lam * sqrt(mx * mx + my * my)) / ((double)N * total));
+    const double pref64 = exp(-lam * sqrt(mx * mx + my * my)) / ((double)N * total);
+    const float pref = (float)pref64;
     float w;
-    if (blk == 0)
+    double w64;
+    if (blk == 0) {
       w = (W[(size_t)(1 * N + r) * d + a] - W[(size_t)(1 * N + nr) * d + a]) / 2.0f;
-    else if (blk == 1)
+      w64 = ((double)W[(size_t)(1 * N + r) * d + a] - (double)W[(size_t)(1 * N + nr) * d + a]) / 2.0;
+    } else if (blk == 1) {
       w = W[(size_t)r * d + a];
-    else if (blk == 2)
+      w64 = w;
+    } else if (blk == 2) {
       w = -W[(size_t)nr * d + a];
-    else
+      w64 = w;
+    } else {
       w = (W[(size_t)(2 * N + r) * d + a] - W[(size_t)(2 * N + nr) * d + a]) / 2.0f;
+      w64 = ((double)W[(size_t)(2 * N + r) * d + a] - (double)W[(size_t)(2 * N + nr) * d + a]) / 2.0;
+    }
     Wt[e] = w * pref;
+    if (Wt64) Wt64[e] = w64 * pref64;
   }
 }
 
@@ -339,24 +350,28 @@ int launch_hop_count(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs,
                      int32_t* counts, cudaStream_t st) {
   if (batch <= 0) return NH_OK;
   int grid = min(batch, num_sms() * 8);
+  ProfScope prof_scope(NH_K_HOP_COUNT, st);
   hop_kernel<false><<<grid, kNumThreads, 0, st>>>(spins, batch, Lx, Ly, n_dirs, 0.0, 0.0, counts,
-                                                  nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                  nullptr, 0, nullptr, nullptr, nullptr, nullptr,
                                                   nullptr);
   return check_launch("hop_kernel<count>");
 }
 
 int launch_scan_counts(const int32_t* counts, int batch, int64_t* offsets, cudaStream_t st) {
+  ProfScope prof_scope(NH_K_SCAN, st);
   scan_kernel<<<1, 1024, 0, st>>>(counts, batch, offsets);
   return check_launch("scan_kernel");
 }
 
 int launch_hop_emit(const int8_t* spins, int batch, int Lx, int Ly, const nh_hubbard_params& h,
-                    const int64_t* offsets, int32_t* rec, double* hval, int32_t* owner,
-                    int32_t* from, int32_t* to, cudaStream_t st) {
+                    const int64_t* offsets, int64_t cap, int32_t* rec, double* hval,
+                    int32_t* owner, int32_t* from, int32_t* to, cudaStream_t st) {
   if (batch <= 0) return NH_OK;
   int grid = min(batch, num_sms() * 8);
+  ProfScope prof_scope(NH_K_HOP_EMIT, st);
   hop_kernel<true><<<grid, kNumThreads, 0, st>>>(spins, batch, Lx, Ly, h.n_dirs, h.t, h.tp,
-                                                 nullptr, offsets, rec, hval, owner, from, to);
+                                                 nullptr, offsets, cap, rec, hval, owner, from,
+                                                 to);
   return check_launch("hop_kernel<emit>");
 }
 
@@ -366,6 +381,7 @@ int launch_eloc_reduce(const int8_t* spins, const float* sign, const double* log
                        cudaStream_t st) {
   if (batch <= 0) return NH_OK;
   int grid = min((batch + 7) / 8, num_sms() * 16);
+  ProfScope prof_scope(NH_K_ELOC_REDUCE, st);
   eloc_reduce_kernel<<<grid, 256, 0, st>>>(spins, sign, logabs, batch, N, U, offsets, hval,
                                            csign, clogabs, eloc);
   return check_launch("eloc_reduce_kernel");
@@ -376,6 +392,7 @@ int launch_mh_propose(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs
                       cudaStream_t st) {
   if (batch <= 0) return NH_OK;
   int grid = min((batch + 7) / 8, num_sms() * 16);
+  ProfScope prof_scope(NH_K_MH_PROPOSE, st);
   mh_propose_kernel<<<grid, 256, 0, st>>>(spins, batch, Lx, Ly, n_dirs, (uint32_t)seed,
                                           (uint32_t)(seed >> 32), (uint32_t)step,
                                           (uint32_t)((uint64_t)step >> 32), valid, from, to);
@@ -385,6 +402,7 @@ int launch_mh_propose(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs
 int launch_compact(const int32_t* valid, const int32_t* from, const int32_t* to, int batch,
                    int32_t* c_sample, int32_t* c_from, int32_t* c_to, int32_t* c_count,
                    cudaStream_t st) {
+  ProfScope prof_scope(NH_K_COMPACT, st);
   compact_kernel<<<1, 1024, 0, st>>>(valid, from, to, batch, c_sample, c_from, c_to, c_count);
   return check_launch("compact_kernel");
 }
@@ -395,6 +413,7 @@ int launch_mh_accept(int8_t* spins, float* sign, double* logabs, int batch, int 
                      uint64_t seed, int64_t step, int32_t* accepted, cudaStream_t st) {
   if (batch <= 0) return NH_OK;
   int grid = min((batch + 255) / 256, num_sms() * 4);
+  ProfScope prof_scope(NH_K_MH_ACCEPT, st);
   mh_accept_kernel<<<grid, 256, 0, st>>>(spins, sign, logabs, N, c_sample, c_from, c_to, c_count,
                                          psign, plogabs, (uint32_t)seed, (uint32_t)(seed >> 32),
                                          (uint32_t)step, (uint32_t)((uint64_t)step >> 32),
@@ -402,8 +421,10 @@ int launch_mh_accept(int8_t* spins, float* sign, double* logabs, int batch, int 
   return check_launch("mh_accept_kernel");
 }
 
-int launch_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, cudaStream_t st) {
-  wtilde_kernel<<<1, 1024, 0, st>>>(W, theta, Lx, Ly, d, Wt);
+int launch_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, double* Wt64,
+                  cudaStream_t st) {
+  ProfScope prof_scope(NH_K_WTILDE, st);
+  wtilde_kernel<<<1, 1024, 0, st>>>(W, theta, Lx, Ly, d, Wt, Wt64);
   return check_launch("wtilde_kernel");
 }
 

@@ -1,15 +1,18 @@
 // Batched log-Pfaffian (blocked Parlett-Reid LTL^T with partial pivoting), the pairing
 // gather, and the combination of symmetry images.
 //
-// One CTA (256 threads) per antisymmetric n x n matrix, n even, n <= 256, two CTAs per SM at
-// n = 224.  The strict lower triangle lives in shared memory in FP32 (row i at offset
-// i (i - 1) / 2).  Thread t owns physical row t.  A pivot does not move data: it swaps the
-// logical labels of two physical rows (my_log), so the panel needs two block barriers per
-// elimination step.  Panel columns are formed lazily (stored column plus the panel's rank-2
-// terms U V^T - V U^T); at the end of a panel of NB steps the active rows are compacted into a
-// list and the trailing triangle receives the rank-2NB update.  The Pfaffian is the product
-// of the pivots A[k, k+1] times the parity of the relabelling; the product is accumulated in
-// FP64 as mantissa and exponent, logabs = log(mantissa) + exponent log 2.
+// One CTA (256 threads) per antisymmetric n x n matrix, n even, n <= 256; FP32 (two CTAs per
+// SM at n = 224) or FP64 (one CTA per SM, used to recompute ill-conditioned items).  The strict
+// lower triangle lives in shared memory (row i at offset i (i - 1) / 2) and thread t owns
+// physical row t.  A pivot does not move data: it swaps the logical labels of two physical rows,
+// so an elimination step costs two block barriers.  Panel columns are formed lazily (stored
+// column plus the panel's rank-2 terms U V^T - V U^T); at the end of a panel of NB steps the
+// active rows are listed in physical order and the trailing triangle receives the rank-2NB
+// update, one warp per row and one lane per column, the column's U/V in registers and the row's
+// U/V broadcast.  The Pfaffian is the product of the pivots A[k, k+1] times the parity of the
+// relabelling, accumulated in FP64 as mantissa and exponent.  The ratio of the largest to the
+// smallest pivot magnitude estimates the condition number; above cond_tau the item is flagged
+// NH_FLAG_GROWTH (near-nodal) for the FP64 recompute.
 //
 // Replaces fermix.slogpf (code/backflow/models.py:210) and, in the gather mode, the Pallas
 // pairing kernel pfsbp_pairing_fwd (code/backflow/pf_kernel.py:156-190) whose formula it
@@ -23,64 +26,99 @@ namespace nh {
 namespace {
 
 constexpr int kWarps = kNumThreads / 32;
-constexpr float kGrowth = 1.0e4f;  // pivot-growth flag threshold (|col max| / initial max)
+
+template <typename T>
+struct Vec;
+template <>
+struct Vec<float> {
+  static constexpr int k = 4;
+};
+template <>
+struct Vec<double> {
+  static constexpr int k = 2;
+};
+
+__device__ __forceinline__ float tfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double tfma(double a, double b, double c) { return fma(a, b, c); }
+
+__device__ __forceinline__ void ldg16(const float* p, float* o) {
+  float4 v = __ldg(reinterpret_cast<const float4*>(p));
+  o[0] = v.x;
+  o[1] = v.y;
+  o[2] = v.z;
+  o[3] = v.w;
+}
+__device__ __forceinline__ void ldg16(const double* p, double* o) {
+  double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  o[0] = v.x;
+  o[1] = v.y;
+}
+__device__ __forceinline__ void lds16(const float* p, float* o) {
+  float4 v = *reinterpret_cast<const float4*>(p);
+  o[0] = v.x;
+  o[1] = v.y;
+  o[2] = v.z;
+  o[3] = v.w;
+}
+__device__ __forceinline__ void lds16(const double* p, double* o) {
+  double2 v = *reinterpret_cast<const double2*>(p);
+  o[0] = v.x;
+  o[1] = v.y;
+}
 
 struct PfArgs {
   int n;
-  int mode;  // 0: F dense (batch, n, n) in global memory; 1: gather from Y / idx / Wt
+  int mode;  // 0: F dense FP32 (items, n, n) in global memory; 1: gather from Y / idx / Wt
   const float* F;
-  const float* Y;
-  const int32_t* idx;
-  const float* Wt;
-  int Lx, Ly, d;
-  const int32_t* n_cfg_dev;  // device count of configurations (items = count * G) or null
-  int G;
-  int n_items;
-  const float* item_sign;
-  float* sign;
-  double* logabs;
-  int32_t* flags;
+  const void* Y;       // (slots, n, D) of T
+  const int32_t* idx;  // (slots, n)
+  const void* Wt;      // (4, N, D) of T
+  int Lx, Ly;
+  const int32_t* count_dev;  // work count on the device (times count_mult) or null
+  int count_mult;
+  int n_slots;               // host count, upper bound when count_dev is set
+  const int32_t* slot_item;  // slot -> item, null: identity
+  const float* item_sign;    // (items,) or null
+  float* sign;               // (items,)
+  double* logabs;            // (items,)
+  int32_t* flags;            // (items,) or null
+  double cond_tau;           // flag NH_FLAG_GROWTH when max|piv| > cond_tau min|piv| (0: off)
+  int flag_or;               // OR-ed into every written flag
 };
 
 __device__ __forceinline__ int tri_off(int i) { return (i * (i - 1)) >> 1; }
 
-// Element (i, j) of the antisymmetric matrix stored as a strict lower triangle.
-__device__ __forceinline__ float aval(const float* Lw, int i, int j) {
-  return i > j ? Lw[tri_off(i) + j] : (i < j ? -Lw[tri_off(j) + i] : 0.0f);
+template <typename T>
+__device__ __forceinline__ T aval(const T* Lw, int i, int j) {
+  return i > j ? Lw[tri_off(i) + j] : (i < j ? -Lw[tri_off(j) + i] : T(0));
 }
 
-// F[p, q] of the gather for p > q (the stored lower element); the row p features are in
-// registers (yp), the Wt row is gathered by displacement and spin block.
-template <int D>
-__device__ __forceinline__ float pair_value(const float* yp, int sp, int xp, int ypos,
-                                            const float* __restrict__ Yq, int mq, int N, int Lx,
-                                            int Ly, const float* __restrict__ Wt) {
+template <typename T, int D>
+__device__ __forceinline__ T pair_value(const T* yp, int sp, int xp, int ypos,
+                                        const T* __restrict__ Yq, int mq, int N, int Lx, int Ly,
+                                        const T* __restrict__ Wt) {
   const int sq = mq >= N ? 1 : 0;
   const int siteq = mq - sq * N;
   const int xq = siteq / Ly, yq = siteq - xq * Ly;
   int dx = xp - xq, dy = ypos - yq;
   dx += dx < 0 ? Lx : 0;
   dy += dy < 0 ? Ly : 0;
-  const int r = dx * Ly + dy;
-  const float4* w4 = reinterpret_cast<const float4*>(Wt + ((size_t)(2 * sp + sq) * N + r) * D);
-  const float4* q4 = reinterpret_cast<const float4*>(Yq);
-  float acc = 0.0f;
+  const T* wrow = Wt + ((size_t)(2 * sp + sq) * N + dx * Ly + dy) * D;
+  T acc = T(0);
 #pragma unroll
-  for (int a4 = 0; a4 < D / 4; ++a4) {
-    const float4 w = __ldg(w4 + a4);
-    const float4 q = __ldg(q4 + a4);
-    acc = fmaf(yp[4 * a4 + 0] * q.x, w.x, acc);
-    acc = fmaf(yp[4 * a4 + 1] * q.y, w.y, acc);
-    acc = fmaf(yp[4 * a4 + 2] * q.z, w.z, acc);
-    acc = fmaf(yp[4 * a4 + 3] * q.w, w.w, acc);
+  for (int a0 = 0; a0 < D; a0 += Vec<T>::k) {
+    T w[Vec<T>::k], q[Vec<T>::k];
+    ldg16(wrow + a0, w);
+    ldg16(Yq + a0, q);
+#pragma unroll
+    for (int k = 0; k < Vec<T>::k; ++k) acc = tfma(yp[a0 + k] * q[k], w[k], acc);
   }
   return acc;
 }
 
-template <int D>
-__device__ void gather_lower(float* Lw, int n, const float* __restrict__ Y,
-                             const int32_t* __restrict__ idx, const float* __restrict__ Wt,
-                             int Lx, int Ly) {
+template <typename T, int D>
+__device__ void gather_lower(T* Lw, int n, const T* __restrict__ Y, const int32_t* __restrict__ idx,
+                             const T* __restrict__ Wt, int Lx, int Ly) {
   const int N = Lx * Ly;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int p = wid; p < n; p += kWarps) {
@@ -88,63 +126,51 @@ __device__ void gather_lower(float* Lw, int n, const float* __restrict__ Y,
     const int sp = mp >= N ? 1 : 0;
     const int sitep = mp - sp * N;
     const int xp = sitep / Ly, ypos = sitep - xp * Ly;
-    float yp[D];
-    const float4* p4 = reinterpret_cast<const float4*>(Y + (size_t)p * D);
+    T yp[D];
 #pragma unroll
-    for (int a4 = 0; a4 < D / 4; ++a4) {
-      float4 v = __ldg(p4 + a4);
-      yp[4 * a4] = v.x;
-      yp[4 * a4 + 1] = v.y;
-      yp[4 * a4 + 2] = v.z;
-      yp[4 * a4 + 3] = v.w;
-    }
-    float* row = Lw + tri_off(p);
+    for (int a0 = 0; a0 < D; a0 += Vec<T>::k) ldg16(Y + (size_t)p * D + a0, yp + a0);
+    T* row = Lw + tri_off(p);
     for (int q = lane; q < p; q += 32)
-      row[q] = pair_value<D>(yp, sp, xp, ypos, Y + (size_t)q * D, __ldg(idx + q), N, Lx, Ly, Wt);
+      row[q] = pair_value<T, D>(yp, sp, xp, ypos, Y + (size_t)q * D, __ldg(idx + q), N, Lx, Ly, Wt);
   }
 }
 
-template <int NB, int D>
-__global__ void __launch_bounds__(kNumThreads, 2) pfaffian_kernel(PfArgs a) {
+template <typename T, int NB, int D>
+__global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
+    pfaffian_kernel(PfArgs a) {
+  static_assert(NB % Vec<T>::k == 0, "panel width must fill 16-byte vectors");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = a.n;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int tri = tri_off(n);
-  float* Lw = reinterpret_cast<float*>(smem_raw);
-  float* Us = Lw + ((tri + 3) & ~3);  // (n, NB)
-  float* Vs = Us + n * NB;            // (n, NB)
-  int* alist = reinterpret_cast<int*>(Vs + n * NB);  // (n) active physical rows
-  float* rkey = reinterpret_cast<float*>(alist + n);  // (warps) best |value|
-  int* rt = reinterpret_cast<int*>(rkey + kWarps);    // (warps) its physical row
-  float* rval = reinterpret_cast<float*>(rt + kWarps);  // (warps) its signed value
-  int* rlog = reinterpret_cast<int*>(rval + kWarps);    // (warps) its logical label
-  int* misc = rlog + kWarps;  // [0] phys of logical k, [1] phys of logical k+1, [2..] scan
+  T* Lw = reinterpret_cast<T*>(smem_raw);
+  T* Us = Lw + ((tri + 3) & ~3);  // (n, NB)
+  T* Vs = Us + n * NB;            // (n, NB)
+  T* rkey = Vs + n * NB;          // (warps) best |value|
+  T* rval = rkey + kWarps;        // (warps) its signed value
+  int* rt = reinterpret_cast<int*>(rval + kWarps);  // (warps) its physical row
+  int* rlog = rt + kWarps;                          // (warps) its logical label
+  int* alist = rlog + kWarps;                       // (n) active physical rows
+  int* misc = alist + n;  // [0] phys of logical k, [1] phys of logical k+1, [2..] counts
 
-  const int n_items = a.n_cfg_dev ? (*a.n_cfg_dev) * a.G : a.n_items;
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+  const int n_work = a.count_dev ? (*a.count_dev) * a.count_mult : a.n_slots;
+  const T* Ybase = static_cast<const T*>(a.Y);
+  const T* Wt = static_cast<const T*>(a.Wt);
+  for (int slot = blockIdx.x; slot < n_work; slot += gridDim.x) {
+    const int item = a.slot_item ? a.slot_item[slot] : slot;
     __syncthreads();
     if (a.mode == 0) {
       const float* F = a.F + (size_t)item * n * n;
       for (int i = wid; i < n; i += kWarps) {
         const float* src = F + (size_t)i * n;
-        float* dst = Lw + tri_off(i);
-        for (int j = lane; j < i; j += 32) dst[j] = __ldg(src + j);
+        T* dst = Lw + tri_off(i);
+        for (int j = lane; j < i; j += 32) dst[j] = T(__ldg(src + j));
       }
     } else {
-      gather_lower<D>(Lw, n, a.Y + (size_t)item * n * D, a.idx + (size_t)item * n, a.Wt, a.Lx,
-                      a.Ly);
+      gather_lower<T, D>(Lw, n, Ybase + (size_t)slot * n * D, a.idx + (size_t)slot * n, Wt,
+                         a.Lx, a.Ly);
     }
-    // Initial max |A| for the growth flag (block reduction).
-    float amax = 0.0f;
-    for (int e = tid; e < tri; e += kNumThreads) amax = fmaxf(amax, fabsf(Lw[e]));
-#pragma unroll
-    for (int o = 16; o; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-    if (lane == 0) rkey[wid] = amax;
     if (tid == 0) misc[0] = 0;
-    __syncthreads();
-    float a0max = 0.0f;
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) a0max = fmaxf(a0max, rkey[w]);
     __syncthreads();
 
     int my_log = tid < n ? tid : -1;
@@ -152,23 +178,23 @@ __global__ void __launch_bounds__(kNumThreads, 2) pfaffian_kernel(PfArgs a) {
     double mant = 1.0;
     int expo = 0;
     int flag = 0;
-    float colmax = 0.0f;
+    T pmin = T(0), pmax = T(0);
     bool zero = false;
 
     for (int k0 = 0; k0 < n - 1 && !zero; k0 += 2 * NB) {
       const int steps = min(NB, (n - k0) >> 1);
-      float myU[NB], myV[NB];
+      T myU[NB], myV[NB];
 #pragma unroll
       for (int j = 0; j < NB; ++j) {
-        myU[j] = 0.0f;
-        myV[j] = 0.0f;
+        myU[j] = T(0);
+        myV[j] = T(0);
       }
 #pragma unroll
       for (int j = 0; j < NB; ++j) {
         if (j < steps && !zero) {
           const int k = k0 + 2 * j;
           const int ck = misc[0];
-          float c = 0.0f;
+          T c = T(0);
           const bool act = my_log > k;
           if (act) {
             c = aval(Lw, tid, ck);
@@ -176,12 +202,12 @@ __global__ void __launch_bounds__(kNumThreads, 2) pfaffian_kernel(PfArgs a) {
             for (int p = 0; p < NB; ++p)
               if (p < j) c += myU[p] * Vs[ck * NB + p] - myV[p] * Us[ck * NB + p];
           }
-          float key = act ? (isnan(c) ? INFINITY : fabsf(c)) : -1.0f;
+          T key = act ? (isnan(c) ? T(INFINITY) : fabs(c)) : T(-1);
           int bt = tid;
 #pragma unroll
           for (int o = 16; o; o >>= 1) {
-            float ok = __shfl_xor_sync(0xffffffffu, key, o);
-            int ot = __shfl_xor_sync(0xffffffffu, bt, o);
+            const T ok = __shfl_xor_sync(0xffffffffu, key, o);
+            const int ot = __shfl_xor_sync(0xffffffffu, bt, o);
             if (ok > key || (ok == key && ot < bt)) {
               key = ok;
               bt = ot;
@@ -195,33 +221,33 @@ __global__ void __launch_bounds__(kNumThreads, 2) pfaffian_kernel(PfArgs a) {
           }
           if (my_log == k + 1) misc[1] = tid;
           __syncthreads();  // (1) pivot candidates
-          float bk = rkey[0];
+          T bk = rkey[0];
           int r = rt[0], w0 = 0;
 #pragma unroll
           for (int w = 1; w < kWarps; ++w) {
-            float kw = rkey[w];
-            int tw = rt[w];
+            const T kw = rkey[w];
+            const int tw = rt[w];
             if (kw > bk || (kw == bk && tw < r)) {
               bk = kw;
               r = tw;
               w0 = w;
             }
           }
-          const float cr = rval[w0];
+          const T cr = rval[w0];
           const int lr = rlog[w0];
           const int p1 = misc[1];
-          if (!(bk > 0.0f)) {
+          if (!(bk > T(0))) {
             zero = true;  // exactly singular (or empty) column: pf = 0
           } else {
             if (tid == r)
               my_log = k + 1;
             else if (tid == p1)
               my_log = lr;
-            const float piv = -cr;
+            const T piv = -cr;
             const bool live = my_log > k + 1;
-            float u = 0.0f, v = 0.0f;
+            T u = T(0), v = T(0);
             if (live) {
-              float dv = aval(Lw, tid, r);
+              T dv = aval(Lw, tid, r);
 #pragma unroll
               for (int p = 0; p < NB; ++p)
                 if (p < j) dv += myU[p] * Vs[r * NB + p] - myV[p] * Us[r * NB + p];
@@ -237,11 +263,13 @@ __global__ void __launch_bounds__(kNumThreads, 2) pfaffian_kernel(PfArgs a) {
             if (my_log == k + 2) misc[0] = tid;
             if (tid == 0) {
               if (lr != k + 1) sgn = -sgn;
-              if (piv < 0.0f) sgn = -sgn;
+              if (piv < T(0)) sgn = -sgn;
+              const T ap = fabs(piv);
               int e;
-              mant = frexp(mant * (double)fabsf(piv), &e);
+              mant = frexp(mant * (double)ap, &e);
               expo += e;
-              colmax = fmaxf(colmax, bk);
+              pmin = (k == 0 || ap < pmin) ? ap : pmin;
+              pmax = ap > pmax ? ap : pmax;
               if (!isfinite(piv)) flag |= NH_FLAG_NONFINITE;
             }
           }
@@ -249,60 +277,59 @@ __global__ void __launch_bounds__(kNumThreads, 2) pfaffian_kernel(PfArgs a) {
         }
       }
       if (zero) break;
-      // Trailing update over the active rows (physical order), rank 2 * steps.
+      // Trailing update of the active rows: warp <-> row, lane <-> column (32-column blocks).
       const int k_end = k0 + 2 * steps;
       const int m = n - k_end;
       if (m >= 2) {
         const bool on = tid < n && my_log >= k_end;
-        unsigned bal = __ballot_sync(0xffffffffu, on);
+        const unsigned bal = __ballot_sync(0xffffffffu, on);
         if (lane == 0) misc[2 + wid] = __popc(bal);
         __syncthreads();
         int before = 0;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) before += (w < wid) ? misc[2 + w] : 0;
         if (on) alist[before + __popc(bal & ((1u << lane) - 1u))] = tid;
-        __syncthreads();  // (3) active list
-        const int T = (m * (m - 1)) >> 1;
-        const int chunk = (T + kNumThreads - 1) / kNumThreads;
-        int e = tid * chunk;
-        const int e_end = min(T, e + chunk);
-        if (e < e_end) {
-          int ia = (int)((1.0f + sqrtf(1.0f + 8.0f * (float)e)) * 0.5f);
-          while (((ia * (ia - 1)) >> 1) > e) --ia;
-          while (((ia * (ia + 1)) >> 1) <= e) ++ia;
-          int ib = e - ((ia * (ia - 1)) >> 1);
-          int pa = alist[ia];
-          float ua[NB], va[NB];
+        __syncthreads();  // (3) active list in physical order
+        int total = 0;
+        for (int cb = 0; 32 * cb + 1 < m; ++cb) total += m - 32 * cb - 1;
+        int cb = 0, rem = wid, cur_cb = -1, ib = 0, pb = 0;
+        T ub[NB], vb[NB];
 #pragma unroll
-          for (int p = 0; p < NB; ++p) {
-            ua[p] = Us[pa * NB + p];
-            va[p] = Vs[pa * NB + p];
+        for (int p = 0; p < NB; ++p) ub[p] = vb[p] = T(0);
+        for (int pi = wid; pi < total; pi += kWarps, rem += kWarps) {
+          while (rem >= m - 32 * cb - 1) {
+            rem -= m - 32 * cb - 1;
+            ++cb;
           }
-          float* rowp = Lw + tri_off(pa);
-          for (; e < e_end; ++e) {
-            const int pb = alist[ib];
-            float acc = rowp[pb];
+          const int ia = 32 * cb + 1 + rem;
+          if (cb != cur_cb) {
+            cur_cb = cb;
+            ib = 32 * cb + lane;
+            pb = ib < m ? alist[ib] : 0;
+#pragma unroll
+            for (int p = 0; p < NB; ++p) {
+              ub[p] = ib < m ? Us[pb * NB + p] : T(0);
+              vb[p] = ib < m ? Vs[pb * NB + p] : T(0);
+            }
+          }
+          const int pa = alist[ia];
+          T ua[NB], va[NB];
+#pragma unroll
+          for (int p = 0; p < NB; p += Vec<T>::k) {
+            lds16(Us + pa * NB + p, ua + p);
+            lds16(Vs + pa * NB + p, va + p);
+          }
+          if (ib < ia) {
+            T* ptr = Lw + tri_off(pa) + pb;
+            T acc = *ptr;
 #pragma unroll
             for (int p = 0; p < NB; ++p) {
               if (p < steps) {
-                acc = fmaf(ua[p], Vs[pb * NB + p], acc);
-                acc = fmaf(-va[p], Us[pb * NB + p], acc);
+                acc = tfma(ua[p], vb[p], acc);
+                acc = tfma(-va[p], ub[p], acc);
               }
             }
-            rowp[pb] = acc;
-            if (++ib == ia) {
-              ++ia;
-              ib = 0;
-              if (e + 1 < e_end) {
-                pa = alist[ia];
-#pragma unroll
-                for (int p = 0; p < NB; ++p) {
-                  ua[p] = Us[pa * NB + p];
-                  va[p] = Vs[pa * NB + p];
-                }
-                rowp = Lw + tri_off(pa);
-              }
-            }
+            *ptr = acc;
           }
         }
         __syncthreads();  // (4) trailing triangle updated
@@ -319,47 +346,64 @@ __global__ void __launch_bounds__(kNumThreads, 2) pfaffian_kernel(PfArgs a) {
         s *= sgn;
         la = log(mant) + (double)expo * 0.6931471805599453;
         if (!isfinite(la)) flag |= NH_FLAG_NONFINITE;
-        if (a0max > 0.0f && colmax > kGrowth * a0max) flag |= NH_FLAG_GROWTH;
+        if (a.cond_tau > 0.0 && (double)pmax > a.cond_tau * (double)pmin) flag |= NH_FLAG_GROWTH;
       }
       if (s == 0.0f) la = -INFINITY;
       a.sign[item] = s;
       a.logabs[item] = la;
-      if (a.flags) a.flags[item] = flag;
+      if (a.flags) a.flags[item] = flag | a.flag_or;
     }
   }
 }
 
-template <int NB, int D>
-int launch_pf(const PfArgs& a, int items, cudaStream_t st) {
-  const int n = a.n;
-  size_t tri = (size_t)n * (n - 1) / 2;
-  size_t smem = sizeof(float) * (((tri + 3) & ~(size_t)3) + 2 * (size_t)n * NB) +
-                sizeof(int) * (size_t)n + 4 * sizeof(float) * kWarps + sizeof(int) * (2 + kWarps);
-  if (smem > 227 * 1024) return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d needs %zu B smem", n, smem);
+template <typename T, int NB>
+size_t pf_smem(int n) {
+  const size_t tri = (size_t)n * (n - 1) / 2;
+  return sizeof(T) * (((tri + 3) & ~(size_t)3) + 2 * (size_t)n * NB + 2 * kWarps) +
+         sizeof(int) * (2 * kWarps + (size_t)n + 2 + kWarps);
+}
+
+template <typename T, int NB, int D>
+int launch_pf(const PfArgs& a, cudaStream_t st) {
+  const size_t smem = pf_smem<T, NB>(a.n);
+  if (smem > 227 * 1024)
+    return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d needs %zu B of shared memory", a.n, smem);
   static size_t configured = 0;
   if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pfaffian_kernel<NB, D>,
+    cudaError_t e = cudaFuncSetAttribute(pfaffian_kernel<T, NB, D>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return check_cuda(e, "slogpf smem attribute");
     configured = smem;
   }
-  int per_sm = smem <= 113 * 1024 ? 2 : 1;
+  const int per_sm = smem <= 113 * 1024 ? 2 : 1;
   int grid = num_sms() * per_sm;
-  if (grid > items) grid = items;
+  if (grid > a.n_slots) grid = a.n_slots;
   if (grid <= 0) return NH_OK;
-  pfaffian_kernel<NB, D><<<grid, kNumThreads, smem, st>>>(a);
+  ProfScope prof_scope(sizeof(T) == 4 ? NH_K_PFAFFIAN : NH_K_PFAFFIAN64, st);
+  pfaffian_kernel<T, NB, D><<<grid, kNumThreads, smem, st>>>(a);
   return check_launch("pfaffian_kernel");
 }
 
-// NB is the largest panel that keeps two CTAs per SM (<= 113 KB of shared memory).
-template <int D>
-int launch_pf_pick(const PfArgs& a, int items, cudaStream_t st) {
-  const int n = a.n;
-  size_t tri = (size_t)n * (n - 1) / 2 * 4;
-  size_t base = tri + 4 * (size_t)n + 256;
-  if (base + 2 * (size_t)n * 8 * 4 <= 113 * 1024) return launch_pf<8, D>(a, items, st);
-  if (base + 2 * (size_t)n * 6 * 4 <= 113 * 1024) return launch_pf<6, D>(a, items, st);
-  return launch_pf<4, D>(a, items, st);
+// FP32: the widest panel that keeps two CTAs per SM; FP64: one CTA per SM.
+template <typename T, int D>
+int launch_pf_pick(const PfArgs& a, cudaStream_t st) {
+  if constexpr (sizeof(T) == 4) {
+    if (pf_smem<T, 8>(a.n) <= 113 * 1024) return launch_pf<T, 8, D>(a, st);
+    return launch_pf<T, 4, D>(a, st);
+  } else {
+    if (pf_smem<T, 4>(a.n) <= 227 * 1024) return launch_pf<T, 4, D>(a, st);
+    return launch_pf<T, 2, D>(a, st);
+  }
+}
+
+template <typename T>
+int launch_pf_d(const PfArgs& a, int d, cudaStream_t st) {
+  switch (d) {
+    case 8: return launch_pf_pick<T, 8>(a, st);
+    case 16: return launch_pf_pick<T, 16>(a, st);
+    case 32: return launch_pf_pick<T, 32>(a, st);
+    default: return fail(NH_ERR_UNSUPPORTED, "amplitude: d=%d (8, 16 or 32)", d);
+  }
 }
 
 // ------------------------------------------------------------------ standalone gather
@@ -382,11 +426,12 @@ __global__ void __launch_bounds__(kNumThreads) pairing_kernel(const float* __res
       const int xp = sitep / Ly, ypos = sitep - xp * Ly;
       float yp[D];
 #pragma unroll
-      for (int aa = 0; aa < D; ++aa) yp[aa] = __ldg(Yi + (size_t)p * D + aa);
+      for (int a0 = 0; a0 < D; a0 += 4) ldg16(Yi + (size_t)p * D + a0, yp + a0);
       for (int q = lane; q < n; q += 32) {
         float v = 0.0f;
         if (q != p)
-          v = pair_value<D>(yp, sp, xp, ypos, Yi + (size_t)q * D, __ldg(ii + q), N, Lx, Ly, Wt);
+          v = pair_value<float, D>(yp, sp, xp, ypos, Yi + (size_t)q * D, __ldg(ii + q), N, Lx, Ly,
+                                   Wt);
         Fi[(size_t)p * n + q] = v;
       }
     }
@@ -394,6 +439,7 @@ __global__ void __launch_bounds__(kNumThreads) pairing_kernel(const float* __res
 }
 
 // ------------------------------------------------------------------ image combination
+// Also used with G = 1 to copy the per-item results into the caller's arrays.
 __global__ void combine_kernel(const float* __restrict__ sg, const double* __restrict__ la,
                                const int32_t* __restrict__ fl, int G, int n_cfg,
                                const int32_t* n_cfg_dev, float* sign, double* logabs,
@@ -403,70 +449,106 @@ __global__ void combine_kernel(const float* __restrict__ sg, const double* __res
     double m = -INFINITY;
     int f = 0;
     for (int g = 0; g < G; ++g) {
-      float s = sg[(size_t)c * G + g];
-      double l = la[(size_t)c * G + g];
+      const float s = sg[(size_t)c * G + g];
+      const double l = la[(size_t)c * G + g];
       if (s != 0.0f && l > m) m = l;
       if (fl) f |= fl[(size_t)c * G + g];
     }
     double tot = 0.0;
     if (m > -INFINITY)
       for (int g = 0; g < G; ++g) {
-        float s = sg[(size_t)c * G + g];
+        const float s = sg[(size_t)c * G + g];
         if (s != 0.0f) tot += (double)s * exp(la[(size_t)c * G + g] - m);
       }
-    float so = tot > 0.0 ? 1.0f : (tot < 0.0 ? -1.0f : 0.0f);
+    const float so = tot > 0.0 ? 1.0f : (tot < 0.0 ? -1.0f : 0.0f);
     sign[c] = so;
     logabs[c] = so != 0.0f ? log(fabs(tot)) + m - log((double)G) : -INFINITY;
     if (flags) flags[c] = f;
   }
 }
 
+// Ordered list of the items whose flags carry NH_FLAG_GROWTH (single CTA).
+__global__ void __launch_bounds__(1024) flagged_kernel(const int32_t* __restrict__ flags,
+                                                       int n_items, const int32_t* count_dev,
+                                                       int count_mult, int32_t* list,
+                                                       int32_t* count) {
+  __shared__ int wsum[32];
+  __shared__ int carry;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int n = count_dev ? (*count_dev) * count_mult : n_items;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = i < n ? ((flags[i] & NH_FLAG_GROWTH) != 0) : 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, v);
+    if (lane == 0) wsum[wid] = __popc(bal);
+    __syncthreads();
+    if (wid == 0) {
+      int w = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      wsum[lane] = w;
+    }
+    __syncthreads();
+    if (v) list[carry + (wid ? wsum[wid - 1] : 0) + __popc(bal & ((1u << lane) - 1u))] = i;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += wsum[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *count = carry;
+}
+
 }  // namespace
 
-int launch_pfaffian_from_F(const float* F, int n, int batch, float* sign, double* logabs,
-                           int32_t* flags, cudaStream_t st) {
+bool pfaffian64_fits(int n) { return pf_smem<double, 2>(n) <= 227 * 1024; }
+
+int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list,
+                           const int32_t* count, bool fp64, double cond_tau, int flag_or,
+                           float* sign, double* logabs, int32_t* flags, cudaStream_t st) {
   if (n <= 0 || n % 2 || n > kNumThreads)
     return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d must be even and <= %d", n, kNumThreads);
   PfArgs a{};
   a.n = n;
   a.mode = 0;
   a.F = F;
-  a.n_items = batch;
-  a.G = 1;
+  a.n_slots = batch;
+  a.count_dev = count;
+  a.count_mult = 1;
+  a.slot_item = list;
   a.sign = sign;
   a.logabs = logabs;
   a.flags = flags;
-  return launch_pf_pick<16>(a, batch, st);
+  a.cond_tau = cond_tau;
+  a.flag_or = flag_or;
+  return fp64 ? launch_pf_pick<double, 16>(a, st) : launch_pf_pick<float, 16>(a, st);
 }
 
-int launch_pfaffian_gather(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly,
-                           int d, int n, int max_items, const ConfigList* cl,
-                           const float* item_sign, float* sign, double* logabs, int32_t* flags,
-                           cudaStream_t st) {
-  if (n <= 0 || n % 2 || n > kNumThreads)
-    return fail(NH_ERR_UNSUPPORTED, "amplitude: n=%d must be even and <= %d", n, kNumThreads);
+int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st) {
+  if (g.n <= 0 || g.n % 2 || g.n > kNumThreads)
+    return fail(NH_ERR_UNSUPPORTED, "amplitude: n=%d must be even and <= %d", g.n, kNumThreads);
   PfArgs a{};
-  a.n = n;
+  a.n = g.n;
   a.mode = 1;
-  a.Y = Y;
-  a.idx = idx;
-  a.Wt = Wt;
-  a.Lx = Lx;
-  a.Ly = Ly;
-  a.d = d;
-  a.n_cfg_dev = cl ? cl->n_cfg_dev : nullptr;
-  a.G = cl ? cl->G : 1;
-  a.n_items = max_items;
-  a.item_sign = item_sign;
-  a.sign = sign;
-  a.logabs = logabs;
-  a.flags = flags;
-  switch (d) {
-    case 8: return launch_pf_pick<8>(a, max_items, st);
-    case 16: return launch_pf_pick<16>(a, max_items, st);
-    case 32: return launch_pf_pick<32>(a, max_items, st);
-    default: return fail(NH_ERR_UNSUPPORTED, "amplitude: d=%d (8, 16 or 32)", d);
-  }
+  a.Y = g.Y;
+  a.idx = g.idx;
+  a.Wt = g.Wt;
+  a.Lx = g.Lx;
+  a.Ly = g.Ly;
+  a.count_dev = g.count_dev;
+  a.count_mult = g.count_mult;
+  a.n_slots = g.n_slots;
+  a.slot_item = g.slot_item;
+  a.item_sign = g.item_sign;
+  a.sign = g.sign;
+  a.logabs = g.logabs;
+  a.flags = g.flags;
+  a.cond_tau = g.cond_tau;
+  a.flag_or = g.flag_or;
+  return g.fp64 ? launch_pf_d<double>(a, g.d, st) : launch_pf_d<float>(a, g.d, st);
 }
 
 int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
@@ -474,6 +556,7 @@ int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, 
   if (batch <= 0) return NH_OK;
   int grid = num_sms() * 4;
   if (grid > batch) grid = batch;
+  ProfScope prof_scope(NH_K_PAIRING, st);
   switch (d) {
     case 8: pairing_kernel<8><<<grid, kNumThreads, 0, st>>>(Y, idx, Wt, Lx, Ly, n, batch, F); break;
     case 16: pairing_kernel<16><<<grid, kNumThreads, 0, st>>>(Y, idx, Wt, Lx, Ly, n, batch, F); break;
@@ -488,8 +571,16 @@ int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, 
                    cudaStream_t st) {
   if (n_cfg <= 0) return NH_OK;
   int grid = (n_cfg + 255) / 256;
+  ProfScope prof_scope(NH_K_COMBINE, st);
   combine_kernel<<<grid, 256, 0, st>>>(sg, la, fl, G, n_cfg, n_cfg_dev, sign, logabs, flags);
   return check_launch("combine_kernel");
+}
+
+int launch_flagged(const int32_t* flags, int n_items, const int32_t* count_dev, int count_mult,
+                   int32_t* list, int32_t* count, cudaStream_t st) {
+  ProfScope prof_scope(NH_K_FLAGGED, st);
+  flagged_kernel<<<1, 1024, 0, st>>>(flags, n_items, count_dev, count_mult, list, count);
+  return check_launch("flagged_kernel");
 }
 
 }  // namespace nh

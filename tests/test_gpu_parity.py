@@ -1,0 +1,291 @@
+"""GPU parity tests: every CUDA entry point against the FP64 oracle on the same inputs.
+
+Bars: configuration bookkeeping, hop enumeration and Pfaffian signs bit-exact; log|psi| within
+1e-4 absolute of FP64 on the FP32 path; batch-mean local energy within 1e-5 t per site.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import neuralhubbard_b200 as nh
+from neuralhubbard_b200 import _lib
+from oracle import backflow as obf
+from oracle import hubbard as ohub
+from oracle import lattice as olat
+from oracle import pfaffian as opf
+from oracle import projection as oproj
+from oracle import sampler as osam
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+LOG_TOL = 1e-4
+
+
+def host_params(model):
+    p = model.host_params
+    return dict(conv_w=[np.asarray(w, np.float64) for w in p["conv_w"]],
+                conv_b=[np.asarray(b, np.float64) for b in p["conv_b"]],
+                W=np.asarray(p["W"], np.float64), theta=float(p["theta"]),
+                Lx=model.geom.LX, Ly=model.geom.LY)
+
+
+def make_model(L, std=0.02, seed=0, channels=32):
+    N = L * L
+    ne = 7 * N // 16
+    params = nh.init_params(L, L, channels=channels, std=std, seed=seed)
+    return nh.PfaffianBackflow(L, L, ne, ne, params=params)
+
+
+def rand_skew32(rng, n, batch):
+    A = rng.normal(size=(batch, n, n)).astype(np.float32)
+    return A - np.swapaxes(A, 1, 2)
+
+
+@pytest.mark.parametrize("n", [2, 4, 56, 100, 224, 256])
+def test_slogpf_random(n):
+    """Gaussian antisymmetric matrices (condition ~ n^2): plain FP32, and with the FP64
+    recompute of the matrices whose pivot ratio exceeds 100."""
+    rng = np.random.default_rng(n)
+    A = rand_skew32(rng, n, 6)
+    s0, l0 = opf.slogpf(A.astype(np.float64))
+    sg, la, fl = nh.slogpf(torch.from_numpy(A).to(DEV), cond_tau=0.0)
+    assert np.array_equal(sg.cpu().numpy(), s0)
+    assert np.max(np.abs(la.cpu().numpy() - l0)) < (1e-4 if n <= 100 else 1e-3)
+    sg, la, fl = nh.slogpf(torch.from_numpy(A).to(DEV))
+    fl = fl.cpu().numpy()
+    assert np.array_equal(sg.cpu().numpy(), s0)
+    err = np.abs(la.cpu().numpy() - l0)
+    refined = (fl & _lib.FLAG_REFINED) != 0
+    if n <= 224:  # the FP64 triangle fits in shared memory
+        assert np.array_equal(refined, (fl & _lib.FLAG_GROWTH) != 0)
+    else:
+        assert not refined.any()
+    assert np.all(err[refined] < 1e-9)
+    assert np.max(err) < (1e-4 if n <= 100 else 1e-3)
+
+
+def test_slogpf_near_nodal():
+    """Near-nodal matrices (one pivot scaled to ~1e-6 of the others, condition ~1e6) are flagged
+    and recomputed in FP64; sign mismatches must be 0."""
+    rng = np.random.default_rng(77)
+    n, B = 224, 16
+    Q = np.linalg.qr(rng.normal(size=(B, n, n)))[0]  # orthogonal: condition ~ pivot ratio
+    blocks = np.zeros((B, n, n))
+    a = rng.uniform(0.5, 2.0, size=(B, n // 2)) * rng.choice([-1, 1], size=(B, n // 2))
+    a[:, 7] *= 1e-6
+    for k in range(n // 2):
+        blocks[:, 2 * k, 2 * k + 1], blocks[:, 2 * k + 1, 2 * k] = a[:, k], -a[:, k]
+    A = np.einsum("bji,bjk,bkl->bil", Q, blocks, Q).astype(np.float32)
+    A = 0.5 * (A - np.swapaxes(A, 1, 2))
+    s0, l0 = opf.slogpf(A.astype(np.float64))
+    sg, la, fl = nh.slogpf(torch.from_numpy(A).to(DEV))
+    fl = fl.cpu().numpy()
+    assert np.all(fl & _lib.FLAG_REFINED)
+    assert np.array_equal(sg.cpu().numpy(), s0)
+    assert np.max(np.abs(la.cpu().numpy() - l0)) < 1e-6
+
+
+def test_slogpf_singular_and_deterministic():
+    rng = np.random.default_rng(1)
+    A = rand_skew32(rng, 56, 4)
+    A[1] = 0.0
+    A[2, :, 7] = 0.0
+    A[2, 7, :] = 0.0
+    t = torch.from_numpy(A).to(DEV)
+    sg, la, fl = nh.slogpf(t)
+    sg, la, fl = sg.cpu().numpy(), la.cpu().numpy(), fl.cpu().numpy()
+    assert sg[1] == 0 and la[1] == -np.inf and fl[1] & _lib.FLAG_ZERO_PIVOT
+    assert sg[2] == 0 and fl[2] & _lib.FLAG_ZERO_PIVOT
+    sg2, la2, _ = nh.slogpf(t)
+    assert np.array_equal(sg2.cpu().numpy(), sg) and np.array_equal(la2.cpu().numpy(), la)
+
+
+def test_wtilde_and_pairing():
+    model = make_model(8, std=0.3)
+    g = model.geom
+    Wt0 = obf.build_wtilde(model.host_params["W"], float(model.theta), 8, 8, np.float32)
+    Wt = model.Wt.cpu().numpy()
+    assert np.allclose(Wt, Wt0, rtol=1e-6, atol=0)
+    Wt64 = obf.build_wtilde(model.host_params["W"].astype(np.float64), float(model.theta), 8, 8)
+    assert np.allclose(model.Wt64.cpu().numpy(), Wt64, rtol=1e-13, atol=0)
+    rng = np.random.default_rng(3)
+    s = olat.random_configs(rng, 5, g.N, g.n_up, g.n_dn)
+    y = model.features(torch.from_numpy(s).to(DEV))
+    idx = obf.fermion_idx(s)
+    Y = np.take_along_axis(y.cpu().numpy().reshape(5, 2 * g.N, g.d), idx[:, :, None], 1)
+    F = nh.pairing_occ(torch.from_numpy(Y).to(DEV), torch.from_numpy(idx.astype(np.int32)).to(DEV),
+                       model.Wt, g).cpu().numpy()
+    assert np.array_equal(F, -np.swapaxes(F, 1, 2))  # exactly antisymmetric
+    F0 = obf.pairing_occ(Y.astype(np.float64), idx, Wt.astype(np.float64), 8, 8)
+    assert np.allclose(F, F0, rtol=1e-5, atol=1e-6 * np.abs(F0).max())
+
+
+@pytest.mark.parametrize("L", [8, 16])
+def test_cnn_features(L):
+    model = make_model(L, std=0.3, seed=L)
+    g = model.geom
+    s = olat.random_configs(np.random.default_rng(L), 4, g.N, g.n_up, g.n_dn)
+    y = model.features(torch.from_numpy(s).to(DEV)).cpu().numpy()
+    hp = host_params(model)
+    y0 = obf.cnn_forward(s, hp["conv_w"], hp["conv_b"], L, L)
+    assert np.max(np.abs(y - y0)) < 2e-5 * max(1.0, np.abs(y0).max())
+
+
+@pytest.mark.parametrize("L,B,symm", [(8, 16, False), (8, 8, True), (16, 4, False), (16, 2, True)])
+def test_amplitude(L, B, symm):
+    model = make_model(L, std=0.3, seed=1)
+    g = model.geom
+    s = olat.random_configs(np.random.default_rng(10 + L), B, g.N, g.n_up, g.n_dn)
+    state = nh.Variational(model, symm=symm)
+    psi = state(s)
+    sg, la = psi.numpy()
+    s0, l0 = oproj.projected_amplitude(s, host_params(model), symm=symm)
+    assert np.array_equal(sg, s0)
+    assert np.max(np.abs(la - l0)) < LOG_TOL
+
+
+@pytest.mark.parametrize("L,symm", [(8, True), (16, False)])
+def test_amplitude_all_fp64(L, symm):
+    """cond_tau = 1 flags every item, so the whole batch takes the FP64 recompute path."""
+    N = L * L
+    ne = 7 * N // 16
+    params = nh.init_params(L, L, channels=32, std=0.3, seed=5)
+    model = nh.PfaffianBackflow(L, L, ne, ne, params=params, cond_tau=1.0)
+    s = olat.random_configs(np.random.default_rng(31), 3, N, ne, ne)
+    psi = nh.Variational(model, symm=symm)(s)
+    sg, la = psi.numpy()
+    assert np.all(psi.flags.cpu().numpy() & _lib.FLAG_REFINED)
+    s0, l0 = oproj.projected_amplitude(s, host_params(model), symm=symm)
+    assert np.array_equal(sg, s0)
+    assert np.max(np.abs(la - l0)) < 1e-9
+
+
+def test_amplitude_baseline_init_16x16():
+    """The benchmark's own initialisation (weights N(0, 0.02)) at 16x16, 8 images."""
+    model = make_model(16, std=0.02, seed=0)
+    g = model.geom
+    s = olat.random_configs(np.random.default_rng(5), 2, g.N, g.n_up, g.n_dn)
+    sg, la = nh.Variational(model, symm=True)(s).numpy()
+    s0, l0 = oproj.projected_amplitude(s, host_params(model), symm=True)
+    assert np.array_equal(sg, s0)
+    assert np.max(np.abs(la - l0)) < LOG_TOL
+
+
+def test_unfused_path_is_bitwise_equal():
+    """features -> gather -> slogpf equals the fused amplitude entry point bit for bit."""
+    model = make_model(8, std=0.3, seed=4)
+    g = model.geom
+    s = olat.random_configs(np.random.default_rng(6), 6, g.N, g.n_up, g.n_dn)
+    ts = torch.from_numpy(s).to(DEV)
+    y = model.features(ts)
+    idx = torch.from_numpy(obf.fermion_idx(s).astype(np.int32)).to(DEV)
+    Y = torch.gather(y.reshape(6, 2 * g.N, g.d), 1, idx.long()[:, :, None].expand(-1, -1, g.d))
+    F = nh.pairing_occ(Y.contiguous(), idx, model.Wt, g)
+    sg, la, _ = nh.slogpf(F, cond_tau=0.0)
+    model.cond_tau = 0.0
+    psi = nh.Variational(model, symm=False)(ts)
+    assert torch.equal(psi.sign, sg) and torch.equal(psi.logabs, la)
+
+
+@pytest.mark.parametrize("L,n_dirs", [(8, 8), (16, 8), (16, 4)])
+def test_hop_list_bit_exact(L, n_dirs):
+    N = L * L
+    ne = 7 * N // 16
+    s = olat.random_configs(np.random.default_rng(L + n_dirs), 12, N, ne, ne)
+    H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2]) if n_dirs == 8 else nh.Hubbard(8.0, 1.0, 1)
+    counts, offsets, rec, hval = H.hop_list(torch.from_numpy(s).to(DEV), L, L)
+    counts, offsets, rec, hval = (x.cpu().numpy() for x in (counts, offsets, rec, hval))
+    assert np.array_equal(counts, ohub.hop_counts(s, L, L, n_dirs))
+    for b in range(12):
+        fr, to, hv = ohub.hops(s[b], L, L, 1.0, -0.2 if n_dirs == 8 else 0.0, n_dirs)
+        sl = slice(offsets[b], offsets[b + 1])
+        assert np.array_equal(rec[sl, 0], fr) and np.array_equal(rec[sl, 1], to)
+        assert np.array_equal(hval[sl], hv)
+
+
+def test_local_energy_against_fock_hamiltonian():
+    """4x4, 2 + 2 electrons: GPU E_loc equals sum_s' H[s, s'] psi(s') / psi(s) with H from
+    explicit fermion operators (golden fixture)."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "hubbard_4x4.npz"))
+    params = nh.init_params(4, 4, channels=16, std=0.3, seed=9)
+    model = nh.PfaffianBackflow(4, 4, 2, 2, params=params)
+    for symm in (False, True):
+        state = nh.Variational(model, symm=symm)
+        H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2])
+        spins = g["spins"]
+        e = H.Oloc(state, nh.Samples(spins)).cpu().numpy()
+        sg_all, la_all = state(g["conn"]).numpy()
+        sg0, la0 = state(spins).numpy()
+        sgo, _ = oproj.projected_amplitude(spins, host_params(model), symm=symm)
+        off = 0
+        checked = 0
+        for b, cnt in enumerate(g["counts"]):
+            sl = slice(off, off + cnt)
+            off += cnt
+            if sgo[b] == 0:  # symmetry-forbidden: psi_P(s) = 0 exactly, E_loc undefined
+                continue
+            ref = np.sum(g["vals"][sl] * sg_all[sl] * sg0[b] * np.exp(la_all[sl] - la0[b]))
+            assert e[b] == pytest.approx(ref, rel=1e-9, abs=1e-9)
+            checked += 1
+        assert checked >= 40
+
+
+def test_local_energy_vs_oracle():
+    L = 8
+    model = make_model(L, std=0.3, seed=2)
+    g = model.geom
+    s = olat.random_configs(np.random.default_rng(21), 3, g.N, g.n_up, g.n_dn)
+    state = nh.Variational(model, symm=False)
+    H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2])
+    e = H.Oloc(state, nh.Samples(s)).cpu().numpy()
+    hp = host_params(model)
+
+    def amp(c):
+        return oproj.projected_amplitude(c, hp, symm=False)
+
+    e0 = ohub.local_energy(s, amp, L, L, 1.0, -0.2, 8.0)
+    # weights N(0, 0.3) give |E_loc| ~ 100-1000 t: relative bar per sample
+    assert np.max(np.abs(e - e0) / np.abs(e0)) < 2e-5
+
+
+@pytest.mark.parametrize("L,B", [(8, 16), (16, 2)])
+def test_local_energy_baseline_init(L, B):
+    """The benchmark's initialisation (N(0, 0.02)): batch-mean E_loc within 1e-5 t per site."""
+    model = make_model(L, std=0.02, seed=0)
+    g = model.geom
+    s = olat.random_configs(np.random.default_rng(40 + L), B, g.N, g.n_up, g.n_dn)
+    state = nh.Variational(model, symm=False)
+    e = nh.Hubbard(8.0, [1.0, -0.2], [1, 2]).Oloc(state, nh.Samples(s)).cpu().numpy()
+    hp = host_params(model)
+    e0 = ohub.local_energy(s, lambda c: oproj.projected_amplitude(c, hp, symm=False), L, L,
+                           1.0, -0.2, 8.0)
+    assert abs(e.mean() - e0.mean()) / g.N < 1e-5
+
+
+def test_metropolis_bookkeeping_replay():
+    """The GPU sampler's chains equal an oracle replay that uses the same Philox draws and the
+    GPU amplitudes of the proposed configurations (bookkeeping bit-exact)."""
+    L = 8
+    model = make_model(L, std=0.3, seed=3)
+    g = model.geom
+    state = nh.Variational(model, symm=False)
+    s0 = olat.random_configs(np.random.default_rng(7), 48, g.N, g.n_up, g.n_dn)
+    smp = nh.ParticleHop(state, 48, n_neighbor=(1, 2), initial_spins=s0, seed=1234)
+    psi0 = (smp.psi.sign.cpu().numpy().astype(np.float64), smp.psi.logabs.cpu().numpy())
+    smp.run(25)
+    s_gpu = smp.spins.cpu().numpy()
+
+    def amp(c):
+        sg, la = state(c).numpy()
+        return sg.astype(np.float64), la
+
+    s_ref, sg_ref, la_ref, acc = osam.metropolis_steps(s0, psi0, amp, L, L, 1234, 0, 25)
+    assert np.array_equal(s_gpu, s_ref)
+    assert np.array_equal(smp.accepted.cpu().numpy(), acc)
+    assert np.array_equal(smp.psi.logabs.cpu().numpy(), la_ref)
+    # particle numbers conserved
+    assert np.all((s_gpu[:, : g.N] > 0).sum(1) == g.n_up)
+    assert np.all((s_gpu[:, g.N :] > 0).sum(1) == g.n_dn)

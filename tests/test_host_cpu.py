@@ -33,7 +33,8 @@ def test_library_exports_every_header_symbol():
     for s in syms:
         assert hasattr(lib, s), s
     lib.nh_abi_version.restype = ctypes.c_int
-    assert lib.nh_abi_version() == 1
+    want = int(re.search(r"#define NH_ABI_VERSION (\d+)", open(HEADER).read()).group(1))
+    assert lib.nh_abi_version() == want
 
 
 def test_ctypes_table_matches_header():
