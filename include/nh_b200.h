@@ -51,6 +51,9 @@ enum {
  *                The features are the last layer's channels: [0, d) spin up, [d, 2d) spin
  *                down, d = channels / 2.
  * conv_w_packed: the same weights repacked by nh_pack_cnn_weights (read by the kernels).
+ * conv_w_tc:     BF16 hi/lo tensor-core layout from nh_pack_cnn_weights_tc (cnn_mode 1 and 2).
+ * cnn_mode:      0 = FP32 CUDA cores; 1 = tcgen05 BF16; 2 = tcgen05 BF16 x3 (hi*hi + hi*lo +
+ *                lo*hi, near-FP32).  Modes 1 and 2 need a 16x16 lattice, 32 channels, 4 layers.
  * Wt:            FP32 (4, N, d) spin-block table from nh_build_wtilde, blocks [uu, ud, du, dd].
  * Wt64:          the same table in FP64 (nh_build_wtilde), or null to disable the FP64
  *                recompute of ill-conditioned items.
@@ -62,12 +65,15 @@ typedef struct {
   const float* conv_w;
   const float* conv_b;
   const float* conv_w_packed;
+  const void* conv_w_tc;
   const float* Wt;
   const double* Wt64;
   int32_t Lx, Ly;
   int32_t n_up, n_dn;
   int32_t channels;
   int32_t layers;
+  int32_t cnn_mode;
+  int32_t reserved;
   double cond_tau;
 } nh_backflow_params;
 
@@ -103,7 +109,8 @@ enum {
   NH_K_CNN64 = 13,
   NH_K_FLAGGED = 14,
   NH_K_PACK = 15,
-  NH_K_COUNT = 16
+  NH_K_CNN_TC = 16,
+  NH_K_COUNT = 24
 };
 int nh_profile_enable(int on);
 int nh_profile_read(double* ms, int64_t* launches, int n_ids);
@@ -116,6 +123,12 @@ int nh_build_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* W
 /* packed (18 C + 9 C^2 (layers - 1),) = conv_w rearranged per layer as [ci][tap][co]. */
 int nh_pack_cnn_weights(const float* conv_w, int channels, int layers, float* packed,
                         void* stream);
+
+/* Tensor-core weight image (nh_pack_cnn_weights_tc_bytes() bytes): BF16 hi and lo parts in the
+ * K-major core-matrix layout; 32 channels, 4 layers. */
+size_t nh_pack_cnn_weights_tc_bytes(void);
+int nh_pack_cnn_weights_tc(const float* conv_w, int channels, int layers, void* packed,
+                           void* stream);
 
 /* Features y (batch, 2, N, d) of batch configurations (no symmetry image). */
 int nh_cnn_forward(const int8_t* spins, int batch, const nh_backflow_params* p, float* features,

@@ -29,6 +29,7 @@ class BackflowParams(ctypes.Structure):
         ("conv_w", c_void_p),
         ("conv_b", c_void_p),
         ("conv_w_packed", c_void_p),
+        ("conv_w_tc", c_void_p),
         ("Wt", c_void_p),
         ("Wt64", c_void_p),
         ("Lx", ctypes.c_int32),
@@ -37,6 +38,8 @@ class BackflowParams(ctypes.Structure):
         ("n_dn", ctypes.c_int32),
         ("channels", ctypes.c_int32),
         ("layers", ctypes.c_int32),
+        ("cnn_mode", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
         ("cond_tau", c_double),
     ]
 
@@ -57,6 +60,8 @@ SIGNATURES = {
     "nh_build_wtilde": (c_int, [c_void_p, c_float, c_int, c_int, c_int, c_void_p, c_void_p,
                                 c_void_p]),
     "nh_pack_cnn_weights": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
+    "nh_pack_cnn_weights_tc_bytes": (c_size_t, []),
+    "nh_pack_cnn_weights_tc": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "nh_cnn_forward": (c_int, [c_void_p, c_int, P_BF, c_void_p, c_void_p]),
     "nh_pairing_occ": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int,
                                c_void_p, c_void_p]),
@@ -111,9 +116,9 @@ def check(rc: int, what: str) -> None:
 KERNEL_IDS = {
     "cnn": 0, "pfaffian": 1, "pairing": 2, "combine": 3, "hop_count": 4, "scan": 5,
     "hop_emit": 6, "eloc_reduce": 7, "mh_propose": 8, "compact": 9, "mh_accept": 10,
-    "wtilde": 11, "pfaffian64": 12, "cnn64": 13, "flagged": 14, "pack": 15,
+    "wtilde": 11, "pfaffian64": 12, "cnn64": 13, "flagged": 14, "pack": 15, "cnn_tc": 16,
 }
-K_COUNT = 16
+K_COUNT = 24
 
 
 def profile_enable(on: bool) -> None:

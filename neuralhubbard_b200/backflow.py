@@ -148,11 +148,13 @@ class PfaffianBackflow:
 
     def __init__(self, Lx: int, Ly: int, n_up: int, n_dn: int, params: Optional[dict] = None,
                  channels: int = 32, layers: int = 4, seed: int = 0, device="cuda",
-                 cond_tau: float = DEFAULT_COND_TAU):
+                 cond_tau: float = DEFAULT_COND_TAU, cnn_mode: int = 0):
         """``cond_tau``: items whose pivot ratio exceeds it are recomputed end to end in FP64
-        (``0`` keeps every item on the FP32 path)."""
+        (``0`` keeps every item on the FP32 path).  ``cnn_mode``: 0 FP32 CUDA cores, 1 tcgen05
+        BF16, 2 tcgen05 BF16 x3 (near-FP32); modes 1 and 2 need 16x16, 32 channels, 4 layers."""
         self.device = torch.device(device)
         self.cond_tau = float(cond_tau)
+        self.cnn_mode = int(cnn_mode)
         if params is None:
             params = init_params(Lx, Ly, channels, layers, seed=seed)
         self.channels = int(params["conv_w"][0].shape[0])
@@ -170,6 +172,12 @@ class PfaffianBackflow:
         self.conv_w_packed = torch.empty_like(self.conv_w)
         _lib.call("nh_pack_cnn_weights", self.conv_w.data_ptr(), self.channels, self.layers,
                   self.conv_w_packed.data_ptr(), stream_ptr(dev))
+        self.conv_w_tc = None
+        if self.channels == 32 and self.layers == 4:
+            nbytes = _lib.load().nh_pack_cnn_weights_tc_bytes()
+            self.conv_w_tc = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            _lib.call("nh_pack_cnn_weights_tc", self.conv_w.data_ptr(), self.channels,
+                      self.layers, self.conv_w_tc.data_ptr(), stream_ptr(dev))
         self.W = torch.from_numpy(np.asarray(params["W"], np.float32)).to(dev).contiguous()
         self.theta = float(params["theta"])
         self.Wt, self.Wt64 = build_wtilde(self.W, self.theta, self.geom, fp64=True)
@@ -178,9 +186,10 @@ class PfaffianBackflow:
     def c_params(self) -> _lib.BackflowParams:
         g = self.geom
         return _lib.BackflowParams(self.conv_w.data_ptr(), self.conv_b.data_ptr(),
-                                   self.conv_w_packed.data_ptr(), self.Wt.data_ptr(),
-                                   self.Wt64.data_ptr(), g.LX, g.LY, g.n_up, g.n_dn,
-                                   self.channels, self.layers, self.cond_tau)
+                                   self.conv_w_packed.data_ptr(), _ptr(self.conv_w_tc),
+                                   self.Wt.data_ptr(), self.Wt64.data_ptr(), g.LX, g.LY, g.n_up,
+                                   g.n_dn, self.channels, self.layers, self.cnn_mode, 0,
+                                   self.cond_tau)
 
     def features(self, spins: torch.Tensor) -> torch.Tensor:
         """(B, 2, N, d) backflow features of int8 configurations (B, 2N)."""

@@ -90,7 +90,8 @@ size_t pipeline_bytes(int max_items, int n, int d) {
   return align256(it * n * d * sizeof(float)) + align256(it * n * sizeof(int32_t)) +
          align256(it * sizeof(float)) * 2 + align256(it * sizeof(double)) +
          align256(it * sizeof(int32_t)) * 2 + align256(sizeof(int32_t)) +
-         align256(it * n * d * sizeof(double)) + align256(it * n * sizeof(int32_t));
+         align256(it * n * d * sizeof(double)) + align256(it * n * sizeof(int32_t)) +
+         align256(sizeof(int32_t));
 }
 
 PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d) {
@@ -112,6 +113,7 @@ PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d) {
   b.count = reinterpret_cast<int32_t*>(take(sizeof(int32_t)));
   b.Y64 = reinterpret_cast<double*>(take(it * n * d * sizeof(double)));
   b.idx64 = reinterpret_cast<int32_t*>(take(it * n * sizeof(int32_t)));
+  b.err = reinterpret_cast<int32_t*>(take(sizeof(int32_t)));
   return b;
 }
 
@@ -122,8 +124,15 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
   const int n = p.n_up + p.n_dn, d = p.channels / 2;
   const int max_items = cl.n_cfg * cl.G;
   if (max_items <= 0) return NH_OK;
-  CnnLaunch c{&cl, &p, 1, false, nullptr, nullptr, 0, nullptr, b.Y, b.idx, b.item_sign};
-  int rc = launch_cnn(c, st);
+  int rc;
+  if (p.cnn_mode == 1 || p.cnn_mode == 2) {
+    if ((rc = check_cuda(cudaMemsetAsync(b.err, 0, sizeof(int32_t), st), "clear error word")))
+      return rc;
+    rc = launch_cnn_tc(cl, p, p.cnn_mode, b.Y, b.idx, b.item_sign, b.err, st);
+  } else {
+    CnnLaunch c{&cl, &p, 1, false, nullptr, nullptr, 0, nullptr, b.Y, b.idx, b.item_sign};
+    rc = launch_cnn(c, st);
+  }
   if (rc) return rc;
   PfGatherArgs g{b.Y, b.idx, p.Wt, p.Lx, p.Ly, d, n, cl.n_cfg_dev, cl.G, max_items, nullptr,
                  b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, p.cond_tau, 0, false};
@@ -146,8 +155,8 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
 static int check_params(const nh_backflow_params* p) {
   if (!p || !p->conv_w || !p->conv_b || !p->Wt || !p->conv_w_packed)
     return fail(NH_ERR_INVALID, "null parameter pointer (conv_w, conv_b, conv_w_packed, Wt)");
-  if (p->Lx < 3 || p->Ly < 3 || p->Lx * p->Ly > kMaxN)
-    return fail(NH_ERR_UNSUPPORTED, "lattice %dx%d (3 <= L, N <= %d)", p->Lx, p->Ly, kMaxN);
+  if (p->Lx < 3 || p->Ly < 3 || p->Lx > 32 || p->Ly > 32)
+    return fail(NH_ERR_UNSUPPORTED, "lattice %dx%d (3 <= Lx, Ly <= 32)", p->Lx, p->Ly);
   const int n = p->n_up + p->n_dn;
   if (p->n_up < 0 || p->n_dn < 0 || n < 2 || n % 2 || n > kNumThreads)
     return fail(NH_ERR_UNSUPPORTED, "electrons %d + %d (even total <= %d)", p->n_up, p->n_dn,
@@ -156,6 +165,12 @@ static int check_params(const nh_backflow_params* p) {
   if (p->channels % 2 || (d != 8 && d != 16 && d != 32))
     return fail(NH_ERR_UNSUPPORTED, "channels %d (16, 32 or 64)", p->channels);
   if (p->layers < 1 || p->layers > 16) return fail(NH_ERR_UNSUPPORTED, "layers %d", p->layers);
+  if (p->cnn_mode < 0 || p->cnn_mode > 2) return fail(NH_ERR_INVALID, "cnn_mode %d", p->cnn_mode);
+  if (p->cnn_mode && !cnn_tc_supported(*p))
+    return fail(NH_ERR_UNSUPPORTED, "cnn_mode %d needs a 16x16 lattice, 32 channels, 4 layers",
+                p->cnn_mode);
+  if (p->cnn_mode && !p->conv_w_tc) return fail(NH_ERR_INVALID, "cnn_mode %d: conv_w_tc is null",
+                                                p->cnn_mode);
   return NH_OK;
 }
 
@@ -217,12 +232,24 @@ int nh_pack_cnn_weights(const float* conv_w, int channels, int layers, float* pa
   return launch_pack_cnn(conv_w, channels, layers, packed, static_cast<cudaStream_t>(stream));
 }
 
+size_t nh_pack_cnn_weights_tc_bytes(void) { return cnn_tc_packed_bytes(); }
+
+int nh_pack_cnn_weights_tc(const float* conv_w, int channels, int layers, void* packed,
+                           void* stream) {
+  if (!conv_w || !packed) return fail(NH_ERR_INVALID, "pack_cnn_weights_tc: null pointer");
+  if (channels != 32 || layers != 4)
+    return fail(NH_ERR_UNSUPPORTED, "pack_cnn_weights_tc: %d channels, %d layers (32, 4)",
+                channels, layers);
+  return launch_pack_cnn_tc(conv_w, static_cast<uint16_t*>(packed),
+                            static_cast<cudaStream_t>(stream));
+}
+
 int nh_cnn_forward(const int8_t* spins, int batch, const nh_backflow_params* p, float* features,
                    void* stream) {
   if (!p || !p->conv_w_packed || !p->conv_b)
     return fail(NH_ERR_INVALID, "cnn_forward: null parameters");
   if (!spins || !features || batch < 0) return fail(NH_ERR_INVALID, "cnn_forward: bad buffers");
-  if (p->Lx < 3 || p->Ly < 3 || p->Lx * p->Ly > kMaxN)
+  if (p->Lx < 3 || p->Ly < 3 || p->Lx > 32 || p->Ly > 32)
     return fail(NH_ERR_UNSUPPORTED, "cnn_forward: lattice %dx%d", p->Lx, p->Ly);
   ConfigList cl{spins, nullptr, nullptr, nullptr, nullptr, batch, 1};
   CnnLaunch c{&cl, p, 0, false, nullptr, nullptr, 0, features, nullptr, nullptr, nullptr};

@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
   T* bsm = wsm + C * C * 9;    // [co]
   int* simg = reinterpret_cast<int*>(bsm + C);  // (2N) +-1 of the image configuration
   int* occl = simg + M2;       // (2N) ascending occupied modes of the image configuration
-  int* wbuf = occl + M2;       // 32 ints of scan scratch
+  int* wbuf = occl + M2;       // 4 Lx + 32 ints of scan scratch
 
   const int G = a.cl.G;
   const int n_work = a.slot_item ? *a.slot_count
@@ -211,17 +211,8 @@ __global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
     }
     int32_t* idst = a.idx + (int64_t)slot * n;
     for (int p = tid; p < n; p += kNumThreads) idst[p] = occl[p < total ? p : 0];
-    // eta_g: parity of the inversions of (g(a_1), ..., g(a_n)).
-    int par = 0;
-    if (g != 0) {
-      for (int i = tid; i < total; i += kNumThreads) {
-        const int gi = sym_map(occl[i], g, a.Lx, a.Ly, N);
-        int inv = 0;
-        for (int j = i + 1; j < total; ++j) inv += sym_map(occl[j], g, a.Lx, a.Ly, N) < gi;
-        par ^= inv & 1;
-      }
-    }
-    const int odd = __syncthreads_count(par);
+    // eta_g from per-row occupation counts (closed form of the inversion parity).
+    const int odd = image_sign_parity(simg, g, a.Lx, a.Ly, wbuf);
     if (tid == 0) {
       const long long kk = total;
       const int rev = (int)((kk * (kk - 1) / 2) & 1);
@@ -252,7 +243,7 @@ __global__ void pack_kernel(const float* __restrict__ w, int C, int layers, floa
 template <typename T>
 size_t cnn_smem(int N, int C) {
   return sizeof(T) * (2 * (size_t)C * (N + 1) + (size_t)C * C * 9 + C) +
-         sizeof(int) * (4 * (size_t)N + 32);
+         sizeof(int) * (4 * (size_t)N + 4 * 32 + 32);
 }
 
 }  // namespace

@@ -44,6 +44,50 @@ __host__ __device__ __forceinline__ int hop_target_site(int site, int dir, int L
   return x * Ly + y;
 }
 
+// Parity (0 or 1) of eta_g, the fermionic reordering sign of symmetry element g on the image
+// configuration simg (+1 occupied / -1 empty per mode, ascending modes sigma N + x Ly + y).
+// For the reflections x -> -x, y -> -y and the spin swap the inversion count has a closed form:
+// x-flip inverts every pair of occupied sites in distinct rows x1, x2 >= 1, y-flip every pair in
+// one row with y1, y2 >= 1, the spin swap every (up, down) pair.  Block-wide (all threads call
+// it); scratch holds 4 Lx + 4 ints.  Lx <= 32 rows, Ly <= 32 sites per row.
+__device__ __forceinline__ int image_sign_parity(const int* simg, int g, int Lx, int Ly,
+                                                 int* scratch) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int N = Lx * Ly;
+  int* kx = scratch;           // (2, Lx) occupied sites per row
+  int* kpx = scratch + 2 * Lx;  // (2, Lx) occupied sites with y >= 1 per row
+  for (int r = wid; r < 2 * Lx; r += nw) {
+    const int sg = r / Lx, x = r - sg * Lx;
+    const bool occ = lane < Ly && simg[sg * N + x * Ly + lane] > 0;
+    const unsigned b = __ballot_sync(0xffffffffu, occ);
+    if (lane == 0) {
+      kx[r] = __popc(b);
+      kpx[r] = __popc(b & ~1u);
+    }
+  }
+  __syncthreads();
+  int par = 0;
+  if (threadIdx.x == 0 && g != 0) {
+    int nsec[2] = {0, 0};
+    for (int sg = 0; sg < 2; ++sg) {
+      long long S = 0, Q = 0, Y = 0;
+      for (int x = 0; x < Lx; ++x) {
+        const long long k = kx[sg * Lx + x], kp = kpx[sg * Lx + x];
+        nsec[sg] += (int)k;
+        if (x >= 1) {
+          S += k;
+          Q += k * k;
+        }
+        Y += kp * (kp - 1) / 2;
+      }
+      if (g & 1) par ^= (int)(((S * S - Q) / 2) & 1);
+      if (g & 2) par ^= (int)(Y & 1);
+    }
+    if (g & 4) par ^= (nsec[0] * nsec[1]) & 1;
+  }
+  return par;  // meaningful in thread 0
+}
+
 // ------------------------------------------------------------------ Philox4x32-10
 // Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC'11).
 struct u32x4 {
@@ -93,6 +137,7 @@ struct PipelineBuffers {
   int32_t* count;     // (1,) their number
   double* Y64;        // (items, n, d)
   int32_t* idx64;     // (items, n)
+  int32_t* err;       // (1,) device error word of the tensor-core CNN
 };
 
 size_t pipeline_bytes(int max_items, int n, int d);
@@ -147,6 +192,12 @@ int launch_flagged(const int32_t* flags, int n_items, const int32_t* count_dev, 
                    int32_t* list, int32_t* count, cudaStream_t st);
 int launch_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, double* Wt64,
                   cudaStream_t st);
+// Tensor-core CNN (nh_cnn_tc.cu).
+size_t cnn_tc_packed_bytes();
+bool cnn_tc_supported(const nh_backflow_params& p);
+int launch_pack_cnn_tc(const float* conv_w, uint16_t* packed, cudaStream_t st);
+int launch_cnn_tc(const ConfigList& cl, const nh_backflow_params& p, int mode, float* Y,
+                  int32_t* idx, float* item_sign, int32_t* err, cudaStream_t st);
 // Whether the FP64 kernels fit in shared memory (n x n Pfaffian; N sites x C channels CNN).
 bool pfaffian64_fits(int n);
 bool cnn64_fits(int N, int C);

@@ -88,6 +88,10 @@ struct PfArgs {
 
 __device__ __forceinline__ int tri_off(int i) { return (i * (i - 1)) >> 1; }
 
+// Pivot-search key of a magnitude: FP32, rounded up so that no non-zero value becomes zero.
+__device__ __forceinline__ float to_key_float(float x) { return x; }
+__device__ __forceinline__ float to_key_float(double x) { return __double2float_ru(x); }
+
 template <typename T>
 __device__ __forceinline__ T aval(const T* Lw, int i, int j) {
   return i > j ? Lw[tri_off(i) + j] : (i < j ? -Lw[tri_off(j) + i] : T(0));
@@ -130,7 +134,15 @@ __device__ void gather_lower(T* Lw, int n, const T* __restrict__ Y, const int32_
 #pragma unroll
     for (int a0 = 0; a0 < D; a0 += Vec<T>::k) ldg16(Y + (size_t)p * D + a0, yp + a0);
     T* row = Lw + tri_off(p);
-    for (int q = lane; q < p; q += 32)
+    int q = lane;
+    for (; q + 32 < p; q += 64) {  // two independent elements per lane in flight
+      const int mq0 = __ldg(idx + q), mq1 = __ldg(idx + q + 32);
+      const T v0 = pair_value<T, D>(yp, sp, xp, ypos, Y + (size_t)q * D, mq0, N, Lx, Ly, Wt);
+      const T v1 = pair_value<T, D>(yp, sp, xp, ypos, Y + (size_t)(q + 32) * D, mq1, N, Lx, Ly, Wt);
+      row[q] = v0;
+      row[q + 32] = v1;
+    }
+    if (q < p)
       row[q] = pair_value<T, D>(yp, sp, xp, ypos, Y + (size_t)q * D, __ldg(idx + q), N, Lx, Ly, Wt);
   }
 }
@@ -146,12 +158,13 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
   T* Lw = reinterpret_cast<T*>(smem_raw);
   T* Us = Lw + ((tri + 3) & ~3);  // (n, NB)
   T* Vs = Us + n * NB;            // (n, NB)
-  T* rkey = Vs + n * NB;          // (warps) best |value|
-  T* rval = rkey + kWarps;        // (warps) its signed value
-  int* rt = reinterpret_cast<int*>(rval + kWarps);  // (warps) its physical row
-  int* rlog = rt + kWarps;                          // (warps) its logical label
+  T* rval = Vs + n * NB;              // (warps) signed value of each warp's pivot candidate
+  T* pivs = rval + kWarps;            // (n / 2) pivots A[k, k+1], multiplied at the end
+  float* rkey = reinterpret_cast<float*>(pivs + ((n / 2 + 3) & ~3));  // (warps) candidate |value|
+  int* rt = reinterpret_cast<int*>(rkey + kWarps);  // (warps) candidate physical row
+  int* rlog = rt + kWarps;                          // (warps) candidate logical label
   int* alist = rlog + kWarps;                       // (n) active physical rows
-  int* misc = alist + n;  // [0] phys of logical k, [1] phys of logical k+1, [2..] counts
+  int* misc = alist + n;  // [0] phys of logical k, [1] relabel parity, [2..] per-warp counts
 
   const int n_work = a.count_dev ? (*a.count_dev) * a.count_mult : a.n_slots;
   const T* Ybase = static_cast<const T*>(a.Y);
@@ -170,15 +183,14 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
       gather_lower<T, D>(Lw, n, Ybase + (size_t)slot * n * D, a.idx + (size_t)slot * n, Wt,
                          a.Lx, a.Ly);
     }
-    if (tid == 0) misc[0] = 0;
+    if (tid == 0) {
+      misc[0] = 0;
+      misc[1] = 0;
+    }
     __syncthreads();
 
     int my_log = tid < n ? tid : -1;
-    float sgn = 1.0f;
-    double mant = 1.0;
-    int expo = 0;
     int flag = 0;
-    T pmin = T(0), pmax = T(0);
     bool zero = false;
 
     for (int k0 = 0; k0 < n - 1 && !zero; k0 += 2 * NB) {
@@ -202,47 +214,44 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
             for (int p = 0; p < NB; ++p)
               if (p < j) c += myU[p] * Vs[ck * NB + p] - myV[p] * Us[ck * NB + p];
           }
-          T key = act ? (isnan(c) ? T(INFINITY) : fabs(c)) : T(-1);
-          int bt = tid;
+          // Warp max of |c| (rounded up to FP32, NaN as +inf), ties to the lowest row.
+          const float mag = act ? (isnan(c) ? INFINITY : to_key_float(fabs(c))) : -1.0f;
+          float wmax = mag;
 #pragma unroll
-          for (int o = 16; o; o >>= 1) {
-            const T ok = __shfl_xor_sync(0xffffffffu, key, o);
-            const int ot = __shfl_xor_sync(0xffffffffu, bt, o);
-            if (ok > key || (ok == key && ot < bt)) {
-              key = ok;
-              bt = ot;
-            }
-          }
-          if (tid == bt) {
-            rkey[wid] = key;
-            rt[wid] = bt;
+          for (int o = 16; o; o >>= 1) wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
+          const unsigned hit = __ballot_sync(0xffffffffu, mag == wmax);
+          if (lane == __ffs(hit) - 1) {
+            rkey[wid] = wmax;
+            rt[wid] = tid;
             rval[wid] = c;
             rlog[wid] = my_log;
           }
-          if (my_log == k + 1) misc[1] = tid;
           __syncthreads();  // (1) pivot candidates
-          T bk = rkey[0];
-          int r = rt[0], w0 = 0;
+          float kw[kWarps];
 #pragma unroll
-          for (int w = 1; w < kWarps; ++w) {
-            const T kw = rkey[w];
-            const int tw = rt[w];
-            if (kw > bk || (kw == bk && tw < r)) {
-              bk = kw;
-              r = tw;
-              w0 = w;
-            }
+          for (int w = 0; w < kWarps; w += 4) {
+            const float4 q4 = *reinterpret_cast<const float4*>(rkey + w);
+            kw[w] = q4.x;
+            kw[w + 1] = q4.y;
+            kw[w + 2] = q4.z;
+            kw[w + 3] = q4.w;
           }
+          float bk = kw[0];
+#pragma unroll
+          for (int w = 1; w < kWarps; ++w) bk = fmaxf(bk, kw[w]);
+          int w0 = kWarps - 1;
+#pragma unroll
+          for (int w = kWarps - 2; w >= 0; --w) w0 = kw[w] == bk ? w : w0;
+          const int r = rt[w0];
           const T cr = rval[w0];
           const int lr = rlog[w0];
-          const int p1 = misc[1];
-          if (!(bk > T(0))) {
+          if (!(bk > 0.0f)) {
             zero = true;  // exactly singular (or empty) column: pf = 0
           } else {
             if (tid == r)
               my_log = k + 1;
-            else if (tid == p1)
-              my_log = lr;
+            else if (my_log == k + 1)
+              my_log = lr;  // the row that held label k+1 takes the pivot's old label
             const T piv = -cr;
             const bool live = my_log > k + 1;
             T u = T(0), v = T(0);
@@ -252,7 +261,7 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
               for (int p = 0; p < NB; ++p)
                 if (p < j) dv += myU[p] * Vs[r * NB + p] - myV[p] * Us[r * NB + p];
               u = dv;
-              v = c / piv;
+              v = c * (T(1) / piv);
             }
             myU[j] = u;
             myV[j] = v;
@@ -262,15 +271,8 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
             }
             if (my_log == k + 2) misc[0] = tid;
             if (tid == 0) {
-              if (lr != k + 1) sgn = -sgn;
-              if (piv < T(0)) sgn = -sgn;
-              const T ap = fabs(piv);
-              int e;
-              mant = frexp(mant * (double)ap, &e);
-              expo += e;
-              pmin = (k == 0 || ap < pmin) ? ap : pmin;
-              pmax = ap > pmax ? ap : pmax;
-              if (!isfinite(piv)) flag |= NH_FLAG_NONFINITE;
+              pivs[k >> 1] = piv;
+              if (lr != k + 1) misc[1] ^= 1;
             }
           }
           __syncthreads();  // (2) panel column written, next column's owner known
@@ -290,63 +292,107 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
         for (int w = 0; w < kWarps; ++w) before += (w < wid) ? misc[2 + w] : 0;
         if (on) alist[before + __popc(bal & ((1u << lane) - 1u))] = tid;
         __syncthreads();  // (3) active list in physical order
+        // Work units: (64-column block cb, group of RT consecutive rows below its diagonal);
+        // lane l updates columns 64 cb + l and 64 cb + 32 + l, so each row's broadcast U/V
+        // serves 64 elements.  All loads of a unit precede its stores (stores may alias loads).
+        constexpr int RT = sizeof(T) == 4 ? 2 : 1;
         int total = 0;
-        for (int cb = 0; 32 * cb + 1 < m; ++cb) total += m - 32 * cb - 1;
-        int cb = 0, rem = wid, cur_cb = -1, ib = 0, pb = 0;
-        T ub[NB], vb[NB];
+        for (int cb = 0; 64 * cb + 1 < m; ++cb) total += (m - 64 * cb - 1 + RT - 1) / RT;
+        int cb = 0, rem = wid, cur_cb = -1, ib0 = 0, ib1 = 0, pb0 = 0, pb1 = 0;
+        T ub0[NB], vb0[NB], ub1[NB], vb1[NB];
 #pragma unroll
-        for (int p = 0; p < NB; ++p) ub[p] = vb[p] = T(0);
+        for (int p = 0; p < NB; ++p) ub0[p] = vb0[p] = ub1[p] = vb1[p] = T(0);
         for (int pi = wid; pi < total; pi += kWarps, rem += kWarps) {
-          while (rem >= m - 32 * cb - 1) {
-            rem -= m - 32 * cb - 1;
+          while (rem >= (m - 64 * cb - 1 + RT - 1) / RT) {
+            rem -= (m - 64 * cb - 1 + RT - 1) / RT;
             ++cb;
           }
-          const int ia = 32 * cb + 1 + rem;
+          const int ia0 = 64 * cb + 1 + rem * RT;
           if (cb != cur_cb) {
             cur_cb = cb;
-            ib = 32 * cb + lane;
-            pb = ib < m ? alist[ib] : 0;
+            ib0 = 64 * cb + lane;
+            ib1 = ib0 + 32;
+            pb0 = ib0 < m ? alist[ib0] : 0;
+            pb1 = ib1 < m ? alist[ib1] : 0;
 #pragma unroll
             for (int p = 0; p < NB; ++p) {
-              ub[p] = ib < m ? Us[pb * NB + p] : T(0);
-              vb[p] = ib < m ? Vs[pb * NB + p] : T(0);
+              ub0[p] = ib0 < m ? Us[pb0 * NB + p] : T(0);
+              vb0[p] = ib0 < m ? Vs[pb0 * NB + p] : T(0);
+              ub1[p] = ib1 < m ? Us[pb1 * NB + p] : T(0);
+              vb1[p] = ib1 < m ? Vs[pb1 * NB + p] : T(0);
             }
           }
-          const int pa = alist[ia];
-          T ua[NB], va[NB];
+          T acc0[RT], acc1[RT], ua[RT][NB], va[RT][NB];
+          int off[RT];
+          bool ok0[RT], ok1[RT];
 #pragma unroll
-          for (int p = 0; p < NB; p += Vec<T>::k) {
-            lds16(Us + pa * NB + p, ua + p);
-            lds16(Vs + pa * NB + p, va + p);
+          for (int rr = 0; rr < RT; ++rr) {
+            const int ia = ia0 + rr;
+            ok0[rr] = ia < m && ib0 < ia;
+            ok1[rr] = ia < m && ib1 < ia;
+            const int pa = alist[ia < m ? ia : ia0];
+            off[rr] = tri_off(pa);
+#pragma unroll
+            for (int p = 0; p < NB; p += Vec<T>::k) {
+              lds16(Us + pa * NB + p, ua[rr] + p);
+              lds16(Vs + pa * NB + p, va[rr] + p);
+            }
           }
-          if (ib < ia) {
-            T* ptr = Lw + tri_off(pa) + pb;
-            T acc = *ptr;
 #pragma unroll
-            for (int p = 0; p < NB; ++p) {
-              if (p < steps) {
-                acc = tfma(ua[p], vb[p], acc);
-                acc = tfma(-va[p], ub[p], acc);
+          for (int rr = 0; rr < RT; ++rr) {
+            acc0[rr] = ok0[rr] ? Lw[off[rr] + pb0] : T(0);
+            acc1[rr] = ok1[rr] ? Lw[off[rr] + pb1] : T(0);
+          }
+#pragma unroll
+          for (int p = 0; p < NB; ++p) {
+            if (p < steps) {
+#pragma unroll
+              for (int rr = 0; rr < RT; ++rr) {
+                acc0[rr] = tfma(ua[rr][p], vb0[p], acc0[rr]);
+                acc1[rr] = tfma(ua[rr][p], vb1[p], acc1[rr]);
+                acc0[rr] = tfma(-va[rr][p], ub0[p], acc0[rr]);
+                acc1[rr] = tfma(-va[rr][p], ub1[p], acc1[rr]);
               }
             }
-            *ptr = acc;
+          }
+#pragma unroll
+          for (int rr = 0; rr < RT; ++rr) {
+            if (ok0[rr]) Lw[off[rr] + pb0] = acc0[rr];
+            if (ok1[rr]) Lw[off[rr] + pb1] = acc1[rr];
           }
         }
         __syncthreads();  // (4) trailing triangle updated
       }
     }
     if (tid == 0) {
+      // Pfaffian = relabelling parity x product of the pivots, accumulated in FP64 as mantissa
+      // and exponent; the pivot ratio flags near-nodal blocks.
       float s = a.item_sign ? a.item_sign[item] : 1.0f;
       double la;
+      if (isnan(s)) flag |= NH_FLAG_NONFINITE;  // the CNN could not compute this item
       if (zero) {
         s = 0.0f;
         la = -INFINITY;
         flag |= NH_FLAG_ZERO_PIVOT;
       } else {
-        s *= sgn;
+        if (misc[1]) s = -s;
+        double mant = 1.0;
+        int expo = 0;
+        double pmin = INFINITY, pmax = 0.0;
+        for (int k = 0; k < n / 2; ++k) {
+          const double pv = (double)pivs[k];
+          if (pv < 0.0) s = -s;
+          const double ap = fabs(pv);
+          if (!isfinite(ap)) flag |= NH_FLAG_NONFINITE;
+          pmin = fmin(pmin, ap);
+          pmax = fmax(pmax, ap);
+          int e;
+          mant = frexp(mant * ap, &e);
+          expo += e;
+        }
         la = log(mant) + (double)expo * 0.6931471805599453;
         if (!isfinite(la)) flag |= NH_FLAG_NONFINITE;
-        if (a.cond_tau > 0.0 && (double)pmax > a.cond_tau * (double)pmin) flag |= NH_FLAG_GROWTH;
+        if (a.cond_tau > 0.0 && pmax > a.cond_tau * pmin) flag |= NH_FLAG_GROWTH;
       }
       if (s == 0.0f) la = -INFINITY;
       a.sign[item] = s;
@@ -359,8 +405,9 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
 template <typename T, int NB>
 size_t pf_smem(int n) {
   const size_t tri = (size_t)n * (n - 1) / 2;
-  return sizeof(T) * (((tri + 3) & ~(size_t)3) + 2 * (size_t)n * NB + 2 * kWarps) +
-         sizeof(int) * (2 * kWarps + (size_t)n + 2 + kWarps);
+  return sizeof(T) * (((tri + 3) & ~(size_t)3) + 2 * (size_t)n * NB + kWarps +
+                      ((n / 2 + 3) & ~(size_t)3)) +
+         sizeof(float) * kWarps + sizeof(int) * (2 * kWarps + (size_t)n + 2 + kWarps);
 }
 
 template <typename T, int NB, int D>

@@ -161,6 +161,25 @@ def test_amplitude_all_fp64(L, symm):
     assert np.max(np.abs(la - l0)) < 1e-9
 
 
+@pytest.mark.parametrize("std,symm", [(0.3, False), (0.02, True)])
+def test_amplitude_tensor_core_cnn(std, symm):
+    """tcgen05 CNN.  BF16 x3 (mode 2) carries ~16 significant bits per feature: it meets the
+    1e-4 bar with the benchmark's weights (std 0.02) and stays within 1e-3 with rough test weights
+    (std 0.3); BF16 (mode 1) is the low-precision form.  Signs must match the oracle."""
+    L, ne = 16, 112
+    params = nh.init_params(L, L, channels=32, std=std, seed=6)
+    s = olat.random_configs(np.random.default_rng(52), 3, L * L, ne, ne)
+    m0 = nh.PfaffianBackflow(L, L, ne, ne, params=params, cnn_mode=0)
+    s0, l0 = oproj.projected_amplitude(s, host_params(m0), symm=symm)
+    for mode, tol in ((2, LOG_TOL if std < 0.1 else 1e-3), (1, 5e-2 if std < 0.1 else 0.5)):
+        m = nh.PfaffianBackflow(L, L, ne, ne, params=params, cnn_mode=mode)
+        psi = nh.Variational(m, symm=symm)(s)
+        sg, la = psi.numpy()
+        assert not (psi.flags.cpu().numpy() & _lib.FLAG_NONFINITE).any()
+        assert np.array_equal(sg, s0), mode
+        assert np.max(np.abs(la - l0)) < tol, (mode, np.max(np.abs(la - l0)))
+
+
 def test_amplitude_baseline_init_16x16():
     """The benchmark's own initialisation (weights N(0, 0.02)) at 16x16, 8 images."""
     model = make_model(16, std=0.02, seed=0)
@@ -227,8 +246,9 @@ def test_local_energy_against_fock_hamiltonian():
             off += cnt
             if sgo[b] == 0:  # symmetry-forbidden: psi_P(s) = 0 exactly, E_loc undefined
                 continue
-            ref = np.sum(g["vals"][sl] * sg_all[sl] * sg0[b] * np.exp(la_all[sl] - la0[b]))
-            assert e[b] == pytest.approx(ref, rel=1e-9, abs=1e-9)
+            terms = g["vals"][sl] * sg_all[sl] * sg0[b] * np.exp(la_all[sl] - la0[b])
+            # near-forbidden samples cancel terms of ~1e7 down to O(1): bound by sum |terms|
+            assert abs(e[b] - terms.sum()) <= 1e-12 * np.abs(terms).sum() + 1e-9
             checked += 1
         assert checked >= 40
 
