@@ -147,6 +147,18 @@ size_t nh_slogpf_workspace_bytes(int batch);
 int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, double* logabs,
               int32_t* flags, void* workspace, size_t workspace_bytes, void* stream);
 
+/* nh_slogpf without a workspace (no counterpart in the reference): for callers that hold only
+ * their input and output buffers and cannot allocate device memory (for example a plugin whose
+ * host runtime owns all device memory, or a path where cudaMalloc's possible device
+ * synchronisation is not acceptable).  The FP64 refinement list lives in a static device array of
+ * NH_SLOGPF_NOALLOC_MAX_BATCH + 64 int32 words held by every GPU that loads the library; batch
+ * beyond that limit returns NH_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * address (make it before any stream capture); all calls share the array, so calls that overlap
+ * on the GPU race.  Allocates nothing.  Same results as nh_slogpf. */
+#define NH_SLOGPF_NOALLOC_MAX_BATCH 65536
+int nh_slogpf_noalloc(const float* F, int n, int batch, double cond_tau, float* sign,
+                      double* logabs, int32_t* flags, void* stream);
+
 /* Amplitudes of batch configurations.  n_symm = 1: psi(s); n_symm = 8: the projection onto the
  * trivial representation of Flip(0) Flip(1) SpinInverse, psi_P(s) = 1/8 sum_g eta_g psi(g s). */
 size_t nh_amplitude_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p);
