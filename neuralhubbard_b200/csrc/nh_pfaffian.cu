@@ -158,13 +158,16 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
   T* Lw = reinterpret_cast<T*>(smem_raw);
   T* Us = Lw + ((tri + 3) & ~3);  // (n, NB)
   T* Vs = Us + n * NB;            // (n, NB)
-  T* rval = Vs + n * NB;              // (warps) signed value of each warp's pivot candidate
-  T* pivs = rval + kWarps;            // (n / 2) pivots A[k, k+1], multiplied at the end
-  float* rkey = reinterpret_cast<float*>(pivs + ((n / 2 + 3) & ~3));  // (warps) candidate |value|
-  int* rt = reinterpret_cast<int*>(rkey + kWarps);  // (warps) candidate physical row
+  // FP32: the winner's signed value shares the key slot (its magnitude is the key); FP64 keeps
+  // it separately.  pivs[k/2] = pivot A[k, k+1], negated when that step swapped labels.
+  constexpr int kValSlots = sizeof(T) == 4 ? 0 : kWarps;
+  T* rval = Vs + n * NB;                 // (warps, FP64 only) candidate signed value
+  T* pivs = rval + kValSlots;            // (n / 2) signed pivots, multiplied at the end
+  float* rkey = reinterpret_cast<float*>(pivs + ((n / 2 + 3) & ~3));  // (warps) candidate key
+  int* rt = reinterpret_cast<int*>(rkey + kWarps);  // (warps) candidate row; later ballot counts
   int* rlog = rt + kWarps;                          // (warps) candidate logical label
   int* alist = rlog + kWarps;                       // (n) active physical rows
-  int* misc = alist + n;  // [0] phys of logical k, [1] relabel parity, [2..] per-warp counts
+  int* misc = alist + n;                            // [0] physical row of logical k
 
   const int n_work = a.count_dev ? (*a.count_dev) * a.count_mult : a.n_slots;
   const T* Ybase = static_cast<const T*>(a.Y);
@@ -183,10 +186,7 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
       gather_lower<T, D>(Lw, n, Ybase + (size_t)slot * n * D, a.idx + (size_t)slot * n, Wt,
                          a.Lx, a.Ly);
     }
-    if (tid == 0) {
-      misc[0] = 0;
-      misc[1] = 0;
-    }
+    if (tid == 0) misc[0] = 0;
     __syncthreads();
 
     int my_log = tid < n ? tid : -1;
@@ -223,8 +223,12 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
           if (lane == __ffs(hit) - 1) {
             rkey[wid] = wmax;
             rt[wid] = tid;
-            rval[wid] = c;
-            rlog[wid] = my_log;
+            if constexpr (sizeof(T) == 4)  // FP32: |c| is the key, the sign rides in bit 31
+              rlog[wid] = my_log | (signbit(c) ? (int)0x80000000 : 0);
+            else {
+              rval[wid] = c;
+              rlog[wid] = my_log;
+            }
           }
           __syncthreads();  // (1) pivot candidates
           float kw[kWarps];
@@ -236,6 +240,7 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
             kw[w + 2] = q4.z;
             kw[w + 3] = q4.w;
           }
+
           float bk = kw[0];
 #pragma unroll
           for (int w = 1; w < kWarps; ++w) bk = fmaxf(bk, kw[w]);
@@ -243,8 +248,13 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
 #pragma unroll
           for (int w = kWarps - 2; w >= 0; --w) w0 = kw[w] == bk ? w : w0;
           const int r = rt[w0];
-          const T cr = rval[w0];
-          const int lr = rlog[w0];
+          const int lw = rlog[w0];
+          const int lr = lw & 0x7FFFFFFF;
+          T cr;
+          if constexpr (sizeof(T) == 4)
+            cr = lw < 0 ? -bk : bk;  // a NaN candidate comes back as an infinite pivot
+          else
+            cr = rval[w0];
           if (!(bk > 0.0f)) {
             zero = true;  // exactly singular (or empty) column: pf = 0
           } else {
@@ -270,10 +280,7 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
               Vs[tid * NB + j] = v;
             }
             if (my_log == k + 2) misc[0] = tid;
-            if (tid == 0) {
-              pivs[k >> 1] = piv;
-              if (lr != k + 1) misc[1] ^= 1;
-            }
+            if (tid == 0) pivs[k >> 1] = lr != k + 1 ? -piv : piv;
           }
           __syncthreads();  // (2) panel column written, next column's owner known
         }
@@ -285,11 +292,11 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
       if (m >= 2) {
         const bool on = tid < n && my_log >= k_end;
         const unsigned bal = __ballot_sync(0xffffffffu, on);
-        if (lane == 0) misc[2 + wid] = __popc(bal);
+        if (lane == 0) rt[wid] = __popc(bal);
         __syncthreads();
         int before = 0;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) before += (w < wid) ? misc[2 + w] : 0;
+        for (int w = 0; w < kWarps; ++w) before += (w < wid) ? rt[w] : 0;
         if (on) alist[before + __popc(bal & ((1u << lane) - 1u))] = tid;
         __syncthreads();  // (3) active list in physical order
         // Work units: (64-column block cb, group of RT consecutive rows below its diagonal);
@@ -375,7 +382,6 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
         la = -INFINITY;
         flag |= NH_FLAG_ZERO_PIVOT;
       } else {
-        if (misc[1]) s = -s;
         double mant = 1.0;
         int expo = 0;
         double pmin = INFINITY, pmax = 0.0;
@@ -405,9 +411,10 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
 template <typename T, int NB>
 size_t pf_smem(int n) {
   const size_t tri = (size_t)n * (n - 1) / 2;
-  return sizeof(T) * (((tri + 3) & ~(size_t)3) + 2 * (size_t)n * NB + kWarps +
+  const size_t val_slots = sizeof(T) == 4 ? 0 : kWarps;
+  return sizeof(T) * (((tri + 3) & ~(size_t)3) + 2 * (size_t)n * NB + val_slots +
                       ((n / 2 + 3) & ~(size_t)3)) +
-         sizeof(float) * kWarps + sizeof(int) * (2 * kWarps + (size_t)n + 2 + kWarps);
+         sizeof(float) * kWarps + sizeof(int) * (2 * kWarps + (size_t)n + 1);
 }
 
 template <typename T, int NB, int D>
