@@ -178,7 +178,8 @@ def run_ours(args) -> None:
     multi = init_from_env("nccl") if world > 1 else False
 
     params = nh.init_params(L, L, CHANNELS, LAYERS, std=0.02, seed=0)
-    model = nh.PfaffianBackflow(L, L, NE, NE, params=params, device=dev, cnn_mode=args.cnn_mode)
+    model = nh.PfaffianBackflow(L, L, NE, NE, params=params, device=dev, cnn_mode=args.cnn_mode,
+                                pf_mode=args.pf_mode)
     state = nh.Variational(model, symm=True, max_parallel=BATCH)
     rng = np.random.default_rng(1000 + rank)
     spins_host = torch.from_numpy(nh.random_spins(rng, BATCH, N_SITES, NE, NE)).pin_memory()
@@ -251,7 +252,8 @@ def run_ours(args) -> None:
         per_launch_s = ms / launches / 1e3
         amps_per_launch = BATCH * IMAGES * args.steps / launches
         flop = {"cnn": CNN_FLOP, "cnn_tc": CNN_FLOP,
-                "pfaffian": PFAFFIAN_FLOP + GATHER_FLOP}.get(dom, 0.0)
+                "pfaffian": PFAFFIAN_FLOP + GATHER_FLOP,
+                "pfaffian_tc": PFAFFIAN_FLOP + GATHER_FLOP}.get(dom, 0.0)
         achieved = flop * amps_per_launch / per_launch_s / 1e12
         tb = TRAFFIC_BYTES.get(dom)
         roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": bf16,
@@ -273,8 +275,10 @@ def run_ours(args) -> None:
             "config": {"workload": "projected amplitudes, 16x16 Hubbard lattice, 112+112 "
                                    "electrons, 8192 configurations x 8 images = 65536 "
                                    "Pfaffians of 224x224 per step",
-                       "form": ["plain FP32", "tcgen05 BF16 CNN",
-                                "tcgen05 BF16x3 CNN"][args.cnn_mode],
+                       "form": ["plain FP32 CNN", "tcgen05 BF16 CNN",
+                                "tcgen05 BF16x3 CNN"][args.cnn_mode] + ", " +
+                               ["CUDA-core Pfaffian",
+                                "tensor-memory 3xTF32 Pfaffian"][args.pf_mode],
                        "L": L, "batch": BATCH, "images": IMAGES,
                        "cnn": "4 x periodic 3x3, 32 channels, tanh-GELU, N(0, 0.02)",
                        "l2": "512 MiB written between timed steps, outside the step events",
@@ -327,6 +331,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cnn-mode", type=int, default=0, choices=[0, 1, 2],
                     help="0: FP32 CUDA-core CNN (plain form); 1: tcgen05 BF16; 2: tcgen05 BF16x3")
+    ap.add_argument("--pf-mode", type=int, default=0, choices=[0, 1],
+                    help="0: CUDA-core Pfaffian; 1: matrix in tensor memory, tcgen05 updates")
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="configurations per step (default 8192; smaller only for profiling)")
     args = ap.parse_args()

@@ -16,6 +16,9 @@
  *                           quantax Variational.__call__(spins) -> LogArray (sign, logabs)
  *   nh_local_energy      <- code/quick_start.py:33               H.Oloc(state, Samples(spins, psi))
  *   nh_metropolis_steps  <- code/states.py:397-408               ParticleHop ... sweep()
+ *   nh_metropolis_steps_learned, nh_proposal_*: the learned hop proposal, new (the reference
+ *                           samples with the uniform ParticleHop only); they extend the same
+ *                           sampler call (code/states.py:397-408).
  */
 #ifndef NH_B200_H
 #define NH_B200_H
@@ -54,6 +57,9 @@ enum {
  * conv_w_tc:     BF16 hi/lo tensor-core layout from nh_pack_cnn_weights_tc (cnn_mode 1 and 2).
  * cnn_mode:      0 = FP32 CUDA cores; 1 = tcgen05 BF16; 2 = tcgen05 BF16 x3 (hi*hi + hi*lo +
  *                lo*hi, near-FP32).  Modes 1 and 2 need a 16x16 lattice, 32 channels, 4 layers.
+ * pf_mode:       0 = Pfaffian on CUDA cores (two matrices per SM in shared memory); 1 = matrix
+ *                resident in tensor memory, rank-16 trailing updates as 3xTF32 tcgen05 MMAs
+ *                (one matrix per SM).  The FP64 recompute always uses the CUDA-core kernel.
  * Wt:            FP32 (4, N, d) spin-block table from nh_build_wtilde, blocks [uu, ud, du, dd].
  * Wt64:          the same table in FP64 (nh_build_wtilde), or null to disable the FP64
  *                recompute of ill-conditioned items.
@@ -73,7 +79,7 @@ typedef struct {
   int32_t channels;
   int32_t layers;
   int32_t cnn_mode;
-  int32_t reserved;
+  int32_t pf_mode;
   double cond_tau;
 } nh_backflow_params;
 
@@ -110,6 +116,11 @@ enum {
   NH_K_FLAGGED = 14,
   NH_K_PACK = 15,
   NH_K_CNN_TC = 16,
+  NH_K_PFAFFIAN_TC = 17,
+  NH_K_PROP_SAMPLE = 18,
+  NH_K_PROP_FORWARD = 19,
+  NH_K_PROP_BACKWARD = 20,
+  NH_K_PROP_ADAM = 21,
   NH_K_COUNT = 24
 };
 int nh_profile_enable(int on);
@@ -193,6 +204,54 @@ int nh_metropolis_steps(int8_t* spins, float* sign, double* logabs, int batch, i
                         const nh_backflow_params* p, int n_dirs, uint64_t seed, int64_t step0,
                         int nsteps, int32_t* accepted, void* workspace, size_t workspace_bytes,
                         void* stream);
+
+/* ---- Learned hop proposal ----
+ * A periodic 3x3 CNN 2 -> 16 -> 16 -> 16 (tanh-GELU after layers 1 and 2) on the +-1 occupation
+ * image; output channel c = sigma * 8 + d at site i is the logit of hopping the spin-sigma
+ * electron at site i one step in hop direction d (the direction order of nh_hop_list).  Move
+ * index m = c * N + i.  A move is valid when the electron exists, d < n_dirs and the target site
+ * of the same spin is empty; q(m | s) = softmax over the valid moves.  Parameters: a flat FP32
+ * vector of NH_PROPOSAL_PARAMS values, W1 (16, 2, 3, 3), b1 (16), W2 (16, 16, 3, 3), b2 (16),
+ * W3 (16, 16, 3, 3), b3 (16); the kernels evaluate the BF16 image from nh_proposal_pack. */
+#define NH_PROPOSAL_PARAMS 4944
+typedef struct {
+  const void* weights; /* BF16 (NH_PROPOSAL_PARAMS,) */
+  int32_t Lx, Ly;
+  int32_t n_dirs; /* 4 or 8 */
+  int32_t reserved;
+} nh_proposal_params;
+
+/* BF16 (round to nearest even) image of the FP32 parameters; count = NH_PROPOSAL_PARAMS. */
+int nh_proposal_pack(const float* master, int count, void* weights_bf16, void* stream);
+/* Raw logits (batch, 16, N) FP32 (invalid moves are not masked). */
+int nh_proposal_forward(const int8_t* spins, int batch, const nh_proposal_params* q,
+                        float* logits, void* stream);
+/* One proposal per configuration with the Philox draw of (seed, step, chain) word 0: from/to
+ * modes, valid (0 when no electron can hop) and log q(reverse | s') - log q(move | s). */
+int nh_proposal_sample(const int8_t* spins, int batch, const nh_proposal_params* q,
+                       uint64_t seed, int64_t step, int32_t* from, int32_t* to, int32_t* valid,
+                       float* log_q_ratio, void* stream);
+/* Training: loss = -(1/batch) sum_b weights[b] log q(moves[b] | spins[b]) (records whose move
+ * is not valid contribute nothing) into loss (1,) and its gradient (NH_PROPOSAL_PARAMS,) into
+ * grad, both FP32, summed in a fixed order (deterministic). */
+size_t nh_proposal_backward_workspace_bytes(int batch);
+int nh_proposal_backward(const int8_t* spins, const int32_t* moves, const float* weights,
+                         int batch, const nh_proposal_params* q, float* loss, float* grad,
+                         void* workspace, size_t workspace_bytes, void* stream);
+/* Adam (bias-corrected, step t >= 1) on the FP32 master; refreshes the BF16 image when
+ * weights_bf16 is not null.  The optimiser step of the training loop. */
+int nh_proposal_adam_step(float* master, float* m, float* v, const float* grad, int count,
+                          int64_t t, float lr, float beta1, float beta2, float eps,
+                          void* weights_bf16, void* stream);
+/* Metropolis steps with the learned proposal and the exact Hastings correction: accept when
+ * log u < 2 (log|psi(s')| - log|psi(s)|) + log q(reverse | s') - log q(move | s), u from word 2
+ * of the chain's Philox draw.  Same buffers as nh_metropolis_steps; q's lattice must equal p's. */
+size_t nh_metropolis_learned_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p);
+int nh_metropolis_steps_learned(int8_t* spins, float* sign, double* logabs, int batch,
+                                int n_symm, const nh_backflow_params* p,
+                                const nh_proposal_params* q, uint64_t seed, int64_t step0,
+                                int nsteps, int32_t* accepted, void* workspace,
+                                size_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -10,11 +10,15 @@ Drop-in surface (after ChenAo-Phys/NeuralHubbard's quantax usage):
     eloc = H.Oloc(state, Samples(spins, psi))             # code/quick_start.py:33
     sampler = ParticleHop(state, 8192, n_neighbor=(1, 2)) # code/states.py:397-408
     samples = sampler.sweep()
+
+Learned proposal (new): HopProposal (network, GPU training), training_records (data from plain
+chains) and LearnedHop (Metropolis with the exact Hastings correction).
 """
 
 from ._lib import NativeLibraryError
 from .backflow import PairGeometry, PfaffianBackflow, build_wtilde, init_params, pairing_occ, slogpf
 from .operator import Hubbard
+from .proposal import HopProposal, LearnedHop, training_records
 from .sampler import ParticleHop, random_spins
 from .state import LogArray, Samples, Variational
 
@@ -27,6 +31,9 @@ __all__ = [
     "pairing_occ",
     "slogpf",
     "Hubbard",
+    "HopProposal",
+    "LearnedHop",
+    "training_records",
     "ParticleHop",
     "random_spins",
     "LogArray",

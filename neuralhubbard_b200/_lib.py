@@ -39,7 +39,7 @@ class BackflowParams(ctypes.Structure):
         ("channels", ctypes.c_int32),
         ("layers", ctypes.c_int32),
         ("cnn_mode", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("pf_mode", ctypes.c_int32),
         ("cond_tau", c_double),
     ]
 
@@ -48,8 +48,15 @@ class HubbardParams(ctypes.Structure):
     _fields_ = [("t", c_double), ("tp", c_double), ("U", c_double), ("n_dirs", ctypes.c_int32)]
 
 
+class ProposalParams(ctypes.Structure):
+    _fields_ = [("weights", c_void_p), ("Lx", ctypes.c_int32), ("Ly", ctypes.c_int32),
+                ("n_dirs", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
 P_BF = ctypes.POINTER(BackflowParams)
 P_H = ctypes.POINTER(HubbardParams)
+P_Q = ctypes.POINTER(ProposalParams)
+PROPOSAL_PARAMS = 4944
 
 # name -> (restype, argtypes); every symbol declared in include/nh_b200.h.
 SIGNATURES = {
@@ -82,6 +89,19 @@ SIGNATURES = {
     "nh_metropolis_steps": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, P_BF, c_int,
                                     c_uint64, c_int64, c_int, c_void_p, c_void_p, c_size_t,
                                     c_void_p]),
+    "nh_proposal_pack": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "nh_proposal_forward": (c_int, [c_void_p, c_int, P_Q, c_void_p, c_void_p]),
+    "nh_proposal_sample": (c_int, [c_void_p, c_int, P_Q, c_uint64, c_int64, c_void_p, c_void_p,
+                                   c_void_p, c_void_p, c_void_p]),
+    "nh_proposal_backward_workspace_bytes": (c_size_t, [c_int]),
+    "nh_proposal_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, P_Q, c_void_p,
+                                     c_void_p, c_void_p, c_size_t, c_void_p]),
+    "nh_proposal_adam_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int64,
+                                      c_float, c_float, c_float, c_float, c_void_p, c_void_p]),
+    "nh_metropolis_learned_workspace_bytes": (c_size_t, [c_int, c_int, P_BF]),
+    "nh_metropolis_steps_learned": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, P_BF,
+                                            P_Q, c_uint64, c_int64, c_int, c_void_p, c_void_p,
+                                            c_size_t, c_void_p]),
 }
 
 _lock = threading.Lock()
@@ -119,6 +139,8 @@ KERNEL_IDS = {
     "cnn": 0, "pfaffian": 1, "pairing": 2, "combine": 3, "hop_count": 4, "scan": 5,
     "hop_emit": 6, "eloc_reduce": 7, "mh_propose": 8, "compact": 9, "mh_accept": 10,
     "wtilde": 11, "pfaffian64": 12, "cnn64": 13, "flagged": 14, "pack": 15, "cnn_tc": 16,
+    "pfaffian_tc": 17, "prop_sample": 18, "prop_forward": 19, "prop_backward": 20,
+    "prop_adam": 21,
 }
 K_COUNT = 24
 

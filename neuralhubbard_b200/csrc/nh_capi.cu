@@ -125,9 +125,10 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
   const int max_items = cl.n_cfg * cl.G;
   if (max_items <= 0) return NH_OK;
   int rc;
-  if (p.cnn_mode == 1 || p.cnn_mode == 2) {
+  if (p.cnn_mode == 1 || p.cnn_mode == 2 || p.pf_mode == 1)
     if ((rc = check_cuda(cudaMemsetAsync(b.err, 0, sizeof(int32_t), st), "clear error word")))
       return rc;
+  if (p.cnn_mode == 1 || p.cnn_mode == 2) {
     rc = launch_cnn_tc(cl, p, p.cnn_mode, b.Y, b.idx, b.item_sign, b.err, st);
   } else {
     CnnLaunch c{&cl, &p, 1, false, nullptr, nullptr, 0, nullptr, b.Y, b.idx, b.item_sign};
@@ -136,7 +137,9 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
   if (rc) return rc;
   PfGatherArgs g{b.Y, b.idx, p.Wt, p.Lx, p.Ly, d, n, cl.n_cfg_dev, cl.G, max_items, nullptr,
                  b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, p.cond_tau, 0, false};
-  if ((rc = launch_pfaffian_gather(g, st))) return rc;
+  if ((rc = p.pf_mode == 1 ? launch_pfaffian_tc(g, 1, nullptr, b.err, st)
+                           : launch_pfaffian_gather(g, st)))
+    return rc;
   if (p.Wt64 && p.cond_tau > 0.0 && pfaffian64_fits(n) && cnn64_fits(p.Lx * p.Ly, p.channels)) {
     if ((rc = launch_flagged(b.pf_flags, max_items, cl.n_cfg_dev, cl.G, b.list, b.count, st)))
       return rc;
@@ -171,6 +174,7 @@ static int check_params(const nh_backflow_params* p) {
                 p->cnn_mode);
   if (p->cnn_mode && !p->conv_w_tc) return fail(NH_ERR_INVALID, "cnn_mode %d: conv_w_tc is null",
                                                 p->cnn_mode);
+  if (p->pf_mode < 0 || p->pf_mode > 1) return fail(NH_ERR_INVALID, "pf_mode %d", p->pf_mode);
   return NH_OK;
 }
 
@@ -427,6 +431,7 @@ struct MhLayout {
   int32_t *valid, *from, *to, *c_sample, *c_from, *c_to, *c_count;
   float* psign;
   double* plogabs;
+  float* lqr;  // learned proposal: log q(reverse) - log q(move) per chain
   void* pipe;
   size_t bytes;
 };
@@ -450,6 +455,7 @@ static MhLayout mh_layout(void* ws, int batch, int n_symm, const nh_backflow_par
   L.c_count = reinterpret_cast<int32_t*>(take(4));
   L.psign = reinterpret_cast<float*>(take((size_t)batch * 4));
   L.plogabs = reinterpret_cast<double*>(take((size_t)batch * 8));
+  L.lqr = reinterpret_cast<float*>(take((size_t)batch * 4));
   L.pipe = take(pipeline_bytes(batch * n_symm, n, d));
   L.bytes = off;
   return L;
@@ -489,7 +495,52 @@ int nh_metropolis_steps(int8_t* spins, float* sign, double* logabs, int batch, i
     ConfigList cl{spins, L.c_sample, L.c_from, L.c_to, L.c_count, batch, n_symm};
     if ((rc = run_pipeline(cl, *p, b, L.psign, L.plogabs, nullptr, st))) return rc;
     if ((rc = launch_mh_accept(spins, sign, logabs, batch, N, L.c_sample, L.c_from, L.c_to,
-                               L.c_count, L.psign, L.plogabs, seed, step, accepted, st)))
+                               L.c_count, L.psign, L.plogabs, nullptr, seed, step, accepted,
+                               st)))
+      return rc;
+  }
+  return NH_OK;
+}
+
+size_t nh_metropolis_learned_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p) {
+  return nh_metropolis_workspace_bytes(batch, n_symm, p);
+}
+
+int nh_metropolis_steps_learned(int8_t* spins, float* sign, double* logabs, int batch,
+                                int n_symm, const nh_backflow_params* p,
+                                const nh_proposal_params* q, uint64_t seed, int64_t step0,
+                                int nsteps, int32_t* accepted, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+  int rc = check_params(p);
+  if (rc) return rc;
+  if ((rc = check_proposal(q))) return rc;
+  if (q->Lx != p->Lx || q->Ly != p->Ly)
+    return fail(NH_ERR_INVALID, "metropolis_learned: proposal lattice %dx%d != %dx%d", q->Lx,
+                q->Ly, p->Lx, p->Ly);
+  if (!spins || !sign || !logabs || batch < 0 || nsteps < 0)
+    return fail(NH_ERR_INVALID, "metropolis_learned: bad buffers");
+  if (n_symm != 1 && n_symm != 8)
+    return fail(NH_ERR_INVALID, "metropolis_learned: n_symm %d", n_symm);
+  if (batch == 0 || nsteps == 0) return NH_OK;
+  const size_t need = nh_metropolis_learned_workspace_bytes(batch, n_symm, p);
+  if (!workspace || workspace_bytes < need)
+    return fail(NH_ERR_WORKSPACE, "metropolis_learned: workspace %zu < %zu bytes",
+                workspace_bytes, need);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  MhLayout L = mh_layout(workspace, batch, n_symm, p);
+  const int n = p->n_up + p->n_dn, d = p->channels / 2, N = p->Lx * p->Ly;
+  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, n, d);
+  for (int t = 0; t < nsteps; ++t) {
+    const int64_t step = step0 + t;
+    if ((rc = launch_prop_sample(spins, batch, *q, seed, step, L.valid, L.from, L.to, L.lqr, st)))
+      return rc;
+    if ((rc = launch_compact(L.valid, L.from, L.to, batch, L.c_sample, L.c_from, L.c_to,
+                             L.c_count, st)))
+      return rc;
+    ConfigList cl{spins, L.c_sample, L.c_from, L.c_to, L.c_count, batch, n_symm};
+    if ((rc = run_pipeline(cl, *p, b, L.psign, L.plogabs, nullptr, st))) return rc;
+    if ((rc = launch_mh_accept(spins, sign, logabs, batch, N, L.c_sample, L.c_from, L.c_to,
+                               L.c_count, L.psign, L.plogabs, L.lqr, seed, step, accepted, st)))
       return rc;
   }
   return NH_OK;

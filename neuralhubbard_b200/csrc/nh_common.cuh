@@ -183,6 +183,10 @@ int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list
                            const int32_t* count, bool fp64, double cond_tau, int flag_or,
                            float* sign, double* logabs, int32_t* flags, cudaStream_t st);
 int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st);
+// Tensor-memory Pfaffian (one matrix per SM, trailing updates on tcgen05): mode 1 gathers from
+// g.Y / g.idx / g.Wt (FP32), mode 0 reads dense F (items, n, n) FP32.
+int launch_pfaffian_tc(const PfGatherArgs& g, int mode, const float* F, int32_t* err,
+                       cudaStream_t st);
 int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
                    int n, int batch, float* F, cudaStream_t st);
 int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, int n_cfg,
@@ -225,10 +229,16 @@ int launch_mh_propose(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs
 int launch_compact(const int32_t* valid, const int32_t* from, const int32_t* to, int batch,
                    int32_t* c_sample, int32_t* c_from, int32_t* c_to, int32_t* c_count,
                    cudaStream_t st);
+// Learned proposal (nh_proposal.cu).
+int check_proposal(const nh_proposal_params* q);
+int launch_prop_sample(const int8_t* spins, int batch, const nh_proposal_params& q, uint64_t seed,
+                       int64_t step, int32_t* valid, int32_t* from, int32_t* to, float* lqr,
+                       cudaStream_t st);
 int launch_mh_accept(int8_t* spins, float* sign, double* logabs, int batch, int N,
                      const int32_t* c_sample, const int32_t* c_from, const int32_t* c_to,
                      const int32_t* c_count, const float* psign, const double* plogabs,
-                     uint64_t seed, int64_t step, int32_t* accepted, cudaStream_t st);
+                     const float* lqr, uint64_t seed, int64_t step, int32_t* accepted,
+                     cudaStream_t st);
 
 int num_sms();
 

@@ -263,11 +263,13 @@ __global__ void __launch_bounds__(1024) compact_kernel(const int32_t* valid, con
   if (threadIdx.x == 0) *c_count = carry;
 }
 
-// Accept when u < |psi'/psi|^2, compared as log(u) < 2 (logabs' - logabs) in FP64.
+// Accept when u < |psi'/psi|^2 q(s|s')/q(s'|s), compared as
+// log(u) < 2 (logabs' - logabs) + lqr[b] in FP64 (lqr null: symmetric proposal).
 __global__ void mh_accept_kernel(int8_t* spins, float* sign, double* logabs, int N,
                                  const int32_t* c_sample, const int32_t* c_from,
                                  const int32_t* c_to, const int32_t* c_count,
-                                 const float* psign, const double* plogabs, uint32_t k0,
+                                 const float* psign, const double* plogabs,
+                                 const float* __restrict__ lqr, uint32_t k0,
                                  uint32_t k1, uint32_t step_lo, uint32_t step_hi,
                                  int32_t* accepted) {
   const int cnt = *c_count;
@@ -276,7 +278,7 @@ __global__ void mh_accept_kernel(int8_t* spins, float* sign, double* logabs, int
     u32x4 r = philox4x32_10(u32x4{step_lo, (uint32_t)b, 0u, step_hi}, k0, k1);
     const double u = u32_to_unit(r.z);
     const float sp = psign[i];
-    const double lr2 = 2.0 * (plogabs[i] - logabs[b]);
+    const double lr2 = 2.0 * (plogabs[i] - logabs[b]) + (lqr ? (double)lqr[b] : 0.0);
     const bool acc = sp != 0.0f && (u == 0.0 || log(u) < lr2);
     if (acc) {
       int8_t* s = spins + (size_t)b * 2 * N;
@@ -410,12 +412,13 @@ int launch_compact(const int32_t* valid, const int32_t* from, const int32_t* to,
 int launch_mh_accept(int8_t* spins, float* sign, double* logabs, int batch, int N,
                      const int32_t* c_sample, const int32_t* c_from, const int32_t* c_to,
                      const int32_t* c_count, const float* psign, const double* plogabs,
-                     uint64_t seed, int64_t step, int32_t* accepted, cudaStream_t st) {
+                     const float* lqr, uint64_t seed, int64_t step, int32_t* accepted,
+                     cudaStream_t st) {
   if (batch <= 0) return NH_OK;
   int grid = min((batch + 255) / 256, num_sms() * 4);
   ProfScope prof_scope(NH_K_MH_ACCEPT, st);
   mh_accept_kernel<<<grid, 256, 0, st>>>(spins, sign, logabs, N, c_sample, c_from, c_to, c_count,
-                                         psign, plogabs, (uint32_t)seed, (uint32_t)(seed >> 32),
+                                         psign, plogabs, lqr, (uint32_t)seed, (uint32_t)(seed >> 32),
                                          (uint32_t)step, (uint32_t)((uint64_t)step >> 32),
                                          accepted);
   return check_launch("mh_accept_kernel");

@@ -20,6 +20,8 @@
 // the features formed first, so that F[q, p] = -F[p, q] holds bit for bit.
 #include <math.h>
 
+#include <algorithm>
+
 #include "nh_common.cuh"
 
 namespace nh {
@@ -556,6 +558,384 @@ __global__ void __launch_bounds__(1024) flagged_kernel(const int32_t* __restrict
   if (threadIdx.x == 0) *count = carry;
 }
 
+
+// ------------------------------------------------------------------ tensor-memory Pfaffian
+// The FP32 matrix lives in tensor memory (one matrix per SM: rows 0-127 in lanes 0-127 of
+// columns [0, NP), rows 128-255 in columns [NP, 2 NP), NP = n rounded up to 32); thread t owns
+// row t and reads pivot columns with tcgen05.ld.  The panel is the same relabelling Parlett-Reid
+// as pfaffian_kernel; at the end of each panel of 8 steps the rank-16 update
+// A += U V^T - V U^T runs on the tensor cores as 3xTF32 products (X = X_big + X_small):
+// U_b V_b^T + U_b V_s^T + U_s V_b^T - V_b U_b^T - V_b U_s^T - V_s U_b^T, six kind::tf32 MMAs
+// (M = 128, N = NP, K = 8) per 128-row tile, the minus signs via the A-negate bit of the
+// instruction descriptor.  Rows and columns of eliminated indices carry U = V = 0 and never
+// change again.  The occupied block is gathered into a shared-memory lower triangle first and
+// copied into tensor memory with tcgen05.st.
+
+constexpr int kTcNB = 8;
+constexpr uint32_t kTcCols = 512;
+constexpr long long kTcWaitLimit = 1ll << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // sm_100 descriptor version; no swizzle, base offset 0
+  return d;
+}
+
+// kind::tf32 instruction descriptor: FP32 accumulate, TF32 A and B, K-major, M = 128, N = np.
+__device__ __forceinline__ uint32_t tf32_idesc(int np, bool neg_a) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) |
+         ((uint32_t)(np >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, 1, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc));
+}
+
+__device__ __forceinline__ float tmem_ld1(uint32_t taddr) {
+  uint32_t r;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(r) : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, "
+      "%29, %30, %31, %32};\n" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15])), "r"(__float_as_uint(v[16])), "r"(__float_as_uint(v[17])),
+      "r"(__float_as_uint(v[18])), "r"(__float_as_uint(v[19])), "r"(__float_as_uint(v[20])),
+      "r"(__float_as_uint(v[21])), "r"(__float_as_uint(v[22])), "r"(__float_as_uint(v[23])),
+      "r"(__float_as_uint(v[24])), "r"(__float_as_uint(v[25])), "r"(__float_as_uint(v[26])),
+      "r"(__float_as_uint(v[27])), "r"(__float_as_uint(v[28])), "r"(__float_as_uint(v[29])),
+      "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31])));
+}
+
+__device__ __forceinline__ float tf32_big(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_addr(bar);
+  for (long long it = 0; it < kTcWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Operand arrays (K-major, no swizzle): element (row t, k) of a 256 x 8 TF32 matrix at
+// (k / 4) * 4096 + (t / 8) * 128 + (t % 8) * 16 + (k % 4) * 4 bytes.
+__device__ __forceinline__ int opnd_off(int t, int k) {
+  return (k >> 2) * 1024 + (t >> 3) * 32 + (t & 7) * 4 + (k & 3);  // in floats
+}
+
+template <int D>
+__global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, int32_t* err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = a.n;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tri = tri_off(n);
+  const int NP = (n + 31) & ~31;
+  const int n_tiles = (n + 127) >> 7;
+  float* region = reinterpret_cast<float*>(smem_raw);  // staging triangle, later the operands
+  const int region_floats = max((tri + 31) & ~31, 4 * 2048 + 2 * kNumThreads * kTcNB);
+  float* Ub = region;               // 4 operand arrays of 256 x 8 TF32 (8 KB each)
+  float* Us = region + 2048;
+  float* Vb = region + 4096;
+  float* Vs = region + 6144;
+  float* Uf = region + 8192;        // FP32 copies [row][8] for the in-panel corrections
+  float* Vf = Uf + kNumThreads * kTcNB;
+  float* pivs = region + region_floats;          // (128) signed pivots
+  float* rkey = pivs + 128;                      // (warps)
+  int* rt = reinterpret_cast<int*>(rkey + kWarps);
+  int* rlog = rt + kWarps;
+  int* misc = rlog + kWarps;                     // [0] physical row of logical k, [1] abort
+  uint64_t* bar = reinterpret_cast<uint64_t*>(misc + 4);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    misc[1] = 0;
+  }
+  if (wid == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(tmem_slot)),
+                 "r"(kTcCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t my_col0 = tmem + ((uint32_t)(32 * (wid & 3)) << 16) + (uint32_t)((tid >> 7) * NP);
+  uint32_t phase = 0;
+
+  const int n_work = a.count_dev ? (*a.count_dev) * a.count_mult : a.n_slots;
+  const float* Ybase = static_cast<const float*>(a.Y);
+  const float* Wt = static_cast<const float*>(a.Wt);
+  for (int slot = blockIdx.x; slot < n_work; slot += gridDim.x) {
+    const int item = a.slot_item ? a.slot_item[slot] : slot;
+    if (misc[1]) {  // a wait expired earlier: mark the item instead of computing it
+      if (tid == 0) {
+        a.sign[item] = NAN;
+        a.logabs[item] = NAN;
+        if (a.flags) a.flags[item] = NH_FLAG_NONFINITE | a.flag_or;
+      }
+      continue;
+    }
+    __syncthreads();
+    if (a.mode == 0) {
+      const float* F = a.F + (size_t)item * n * n;
+      for (int i = wid; i < n; i += kWarps) {
+        const float* src = F + (size_t)i * n;
+        float* dst = region + tri_off(i);
+        for (int j = lane; j < i; j += 32) dst[j] = __ldg(src + j);
+      }
+    } else {
+      gather_lower<float, D>(region, n, Ybase + (size_t)slot * n * D, a.idx + (size_t)slot * n,
+                             Wt, a.Lx, a.Ly);
+    }
+    __syncthreads();
+    // Full antisymmetric matrix into tensor memory, 32 columns per store; rows >= n are zero.
+    for (int b = 0; b < NP / 32; ++b) {
+      float v[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const int q = 32 * b + i;
+        float x = 0.0f;
+        if (tid < n && q < n) x = q < tid ? region[tri_off(tid) + q] : (q > tid ? -region[tri_off(q) + tid] : 0.0f);
+        v[i] = x;
+      }
+      tmem_st32(my_col0 + 32 * b, v);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();  // the staging triangle is dead from here: the operand arrays reuse it
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) misc[0] = 0;
+    __syncthreads();
+
+    int my_log = tid < n ? tid : -1;
+    int flag = 0;
+    bool zero = false, abort = false;
+    for (int k0 = 0; k0 < n - 1 && !zero && !abort; k0 += 2 * kTcNB) {
+      const int steps = min(kTcNB, (n - k0) >> 1);
+      float myU[kTcNB], myV[kTcNB];
+#pragma unroll
+      for (int j = 0; j < kTcNB; ++j) {
+        myU[j] = 0.0f;
+        myV[j] = 0.0f;
+        if (j >= steps) {  // columns a short last panel leaves unused must be zero
+          Ub[opnd_off(tid, j)] = 0.0f;
+          Us[opnd_off(tid, j)] = 0.0f;
+          Vb[opnd_off(tid, j)] = 0.0f;
+          Vs[opnd_off(tid, j)] = 0.0f;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kTcNB; ++j) {
+        if (j < steps && !zero) {
+          const int k = k0 + 2 * j;
+          const int ck = misc[0];
+          float c = tmem_ld1(my_col0 + ck);
+          const bool act = my_log > k;
+          if (act) {
+#pragma unroll
+            for (int p = 0; p < kTcNB; ++p)
+              if (p < j) c += myU[p] * Vf[ck * kTcNB + p] - myV[p] * Uf[ck * kTcNB + p];
+          }
+          const float mag = act ? (isnan(c) ? INFINITY : fabsf(c)) : -1.0f;
+          float wmax = mag;
+#pragma unroll
+          for (int o = 16; o; o >>= 1) wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
+          const unsigned hit = __ballot_sync(0xffffffffu, mag == wmax);
+          if (lane == __ffs(hit) - 1) {
+            rkey[wid] = wmax;
+            rt[wid] = tid;
+            rlog[wid] = my_log | (signbit(c) ? (int)0x80000000 : 0);
+          }
+          __syncthreads();  // (1) pivot candidates
+          float kw[kWarps];
+#pragma unroll
+          for (int w = 0; w < kWarps; ++w) kw[w] = rkey[w];
+          float bk = kw[0];
+#pragma unroll
+          for (int w = 1; w < kWarps; ++w) bk = fmaxf(bk, kw[w]);
+          int w0 = kWarps - 1;
+#pragma unroll
+          for (int w = kWarps - 2; w >= 0; --w) w0 = kw[w] == bk ? w : w0;
+          const int r = rt[w0];
+          const int lw = rlog[w0];
+          const int lr = lw & 0x7FFFFFFF;
+          const float cr = lw < 0 ? -bk : bk;
+          if (!(bk > 0.0f)) {
+            zero = true;
+          } else {
+            if (tid == r)
+              my_log = k + 1;
+            else if (my_log == k + 1)
+              my_log = lr;
+            const float piv = -cr;
+            const bool live = my_log > k + 1;
+            float dv = tmem_ld1(my_col0 + r);
+            float u = 0.0f, v = 0.0f;
+            if (live) {
+#pragma unroll
+              for (int p = 0; p < kTcNB; ++p)
+                if (p < j) dv += myU[p] * Vf[r * kTcNB + p] - myV[p] * Uf[r * kTcNB + p];
+              u = dv;
+              v = c * (1.0f / piv);
+            }
+            myU[j] = u;
+            myV[j] = v;
+            Uf[tid * kTcNB + j] = u;
+            Vf[tid * kTcNB + j] = v;
+            // Both parts rounded to TF32 here: the tensor cores would truncate an unrounded
+            // small part, a bias that accumulates over the pivots.
+            const float ub = tf32_big(u), vb = tf32_big(v);
+            Ub[opnd_off(tid, j)] = ub;
+            Us[opnd_off(tid, j)] = tf32_big(u - ub);
+            Vb[opnd_off(tid, j)] = vb;
+            Vs[opnd_off(tid, j)] = tf32_big(v - vb);
+            if (my_log == k + 2) misc[0] = tid;
+            if (tid == 0) pivs[k >> 1] = lr != k + 1 ? -piv : piv;
+          }
+          __syncthreads();  // (2) panel column written, next column's owner known
+        }
+      }
+      if (zero) break;
+      if (n - (k0 + 2 * steps) < 2) break;  // nothing left to update
+      // Rank-16 trailing update on the tensor cores.
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t ub = smem_addr(Ub), us = smem_addr(Us), vb = smem_addr(Vb),
+                       vs = smem_addr(Vs);
+        const uint32_t lbo = 4096, sbo = 128;
+        const uint32_t id_pos = tf32_idesc(NP, false), id_neg = tf32_idesc(NP, true);
+        for (int mt = 0; mt < n_tiles; ++mt) {
+          const uint32_t d = tmem + (uint32_t)(mt * NP);
+          const uint32_t ro = (uint32_t)(mt * 128 / 8 * 128);  // first row group of the tile
+          mma_tf32(d, tc_desc(ub + ro, lbo, sbo), tc_desc(vb, lbo, sbo), id_pos);
+          mma_tf32(d, tc_desc(ub + ro, lbo, sbo), tc_desc(vs, lbo, sbo), id_pos);
+          mma_tf32(d, tc_desc(us + ro, lbo, sbo), tc_desc(vb, lbo, sbo), id_pos);
+          mma_tf32(d, tc_desc(vb + ro, lbo, sbo), tc_desc(ub, lbo, sbo), id_neg);
+          mma_tf32(d, tc_desc(vb + ro, lbo, sbo), tc_desc(us, lbo, sbo), id_neg);
+          mma_tf32(d, tc_desc(vs + ro, lbo, sbo), tc_desc(ub, lbo, sbo), id_neg);
+        }
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_addr(bar))
+            : "memory");
+      }
+      if (!tc_wait(bar, phase)) {
+        if (tid == 0) atomicExch(err, 1);
+        misc[1] = 1;
+      }
+      phase ^= 1u;
+      __syncthreads();
+      abort = misc[1] != 0;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    if (tid == 0) {
+      float s = a.item_sign ? a.item_sign[item] : 1.0f;
+      double la;
+      if (isnan(s)) flag |= NH_FLAG_NONFINITE;
+      if (abort) {
+        s = NAN;
+        la = NAN;
+        flag |= NH_FLAG_NONFINITE;
+      } else if (zero) {
+        s = 0.0f;
+        la = -INFINITY;
+        flag |= NH_FLAG_ZERO_PIVOT;
+      } else {
+        double mant = 1.0;
+        int expo = 0;
+        double pmin = INFINITY, pmax = 0.0;
+        for (int k = 0; k < n / 2; ++k) {
+          const double pv = (double)pivs[k];
+          if (pv < 0.0) s = -s;
+          const double ap = fabs(pv);
+          if (!isfinite(ap)) flag |= NH_FLAG_NONFINITE;
+          pmin = fmin(pmin, ap);
+          pmax = fmax(pmax, ap);
+          int e;
+          mant = frexp(mant * ap, &e);
+          expo += e;
+        }
+        la = log(mant) + (double)expo * 0.6931471805599453;
+        if (!isfinite(la)) flag |= NH_FLAG_NONFINITE;
+        if (a.cond_tau > 0.0 && pmax > a.cond_tau * pmin) flag |= NH_FLAG_GROWTH;
+      }
+      if (s == 0.0f) la = -INFINITY;
+      a.sign[item] = s;
+      a.logabs[item] = la;
+      if (a.flags) a.flags[item] = flag | a.flag_or;
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (wid == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTcCols)
+                 : "memory");
+}
+
+size_t pf_tc_smem(int n) {
+  const size_t tri = (size_t)n * (n - 1) / 2;
+  const size_t region = std::max((tri + 31) & ~(size_t)31,
+                                 (size_t)(4 * 2048 + 2 * kNumThreads * kTcNB));
+  const size_t need = sizeof(float) * (region + 128 + kWarps) + sizeof(int) * (2 * kWarps + 4) + 32;
+  // At least 120 KB, so that two CTAs never share an SM: each allocates all 512 tensor-memory
+  // columns, and a second CTA would stall in tcgen05.alloc until the first one exits.
+  return std::max(need, (size_t)120 * 1024);
+}
+
+template <int D>
+int launch_pf_tc(const PfArgs& a, int32_t* err, cudaStream_t st) {
+  const size_t smem = pf_tc_smem(a.n);
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(pfaffian_tc_kernel<D>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return check_cuda(e, "tensor-memory Pfaffian smem attribute");
+    configured = true;
+  }
+  int grid = num_sms();
+  if (grid > a.n_slots) grid = a.n_slots;
+  if (grid <= 0) return NH_OK;
+  ProfScope prof_scope(NH_K_PFAFFIAN_TC, st);
+  pfaffian_tc_kernel<D><<<grid, kNumThreads, smem, st>>>(a, err);
+  return check_launch("pfaffian_tc_kernel");
+}
 }  // namespace
 
 bool pfaffian64_fits(int n) { return pf_smem<double, 2>(n) <= 227 * 1024; }
@@ -603,6 +983,38 @@ int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st) {
   a.cond_tau = g.cond_tau;
   a.flag_or = g.flag_or;
   return g.fp64 ? launch_pf_d<double>(a, g.d, st) : launch_pf_d<float>(a, g.d, st);
+}
+
+int launch_pfaffian_tc(const PfGatherArgs& g, int mode, const float* F, int32_t* err,
+                       cudaStream_t st) {
+  if (g.n <= 0 || g.n % 2 || g.n > kNumThreads)
+    return fail(NH_ERR_UNSUPPORTED, "tensor-memory Pfaffian: n=%d must be even and <= %d", g.n,
+                kNumThreads);
+  PfArgs a{};
+  a.n = g.n;
+  a.mode = mode;
+  a.F = F;
+  a.Y = g.Y;
+  a.idx = g.idx;
+  a.Wt = g.Wt;
+  a.Lx = g.Lx;
+  a.Ly = g.Ly;
+  a.count_dev = g.count_dev;
+  a.count_mult = g.count_mult;
+  a.n_slots = g.n_slots;
+  a.slot_item = g.slot_item;
+  a.item_sign = g.item_sign;
+  a.sign = g.sign;
+  a.logabs = g.logabs;
+  a.flags = g.flags;
+  a.cond_tau = g.cond_tau;
+  a.flag_or = g.flag_or;
+  switch (mode == 0 ? 16 : g.d) {
+    case 8: return launch_pf_tc<8>(a, err, st);
+    case 16: return launch_pf_tc<16>(a, err, st);
+    case 32: return launch_pf_tc<32>(a, err, st);
+    default: return fail(NH_ERR_UNSUPPORTED, "tensor-memory Pfaffian: d=%d", g.d);
+  }
 }
 
 int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
