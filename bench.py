@@ -11,6 +11,12 @@ evaluations per second over all ranks with the inputs resident in HBM; ``e2e`` i
 metric through the public API with the configurations copied from pinned host memory and the
 amplitudes read back every step.
 
+``sampling`` (1 GPU) compares the plain form (FP32 CNN, uniform-hop Metropolis) with the
+chosen form (tcgen05 BF16x3 CNN, learned hop proposal with the exact Hastings correction,
+trained on 2^20 records of the plain chains): acceptance, tau_int of the log|psi| series,
+effective samples per second and the energy per site of each, on 1024 chains that start from
+the same configurations after 6000 equilibration steps.
+
 Under torchrun each rank evaluates its own 8192 configurations (weak scaling); the time is the
 maximum over ranks of the summed per-step CUDA-event durations.  ``--impl reference`` times the
 CPU restatement of the same path (the reference's JAX stack cannot be installed here) on all
@@ -45,9 +51,10 @@ CNN_FLOP = 2 * 9 * (2 * CHANNELS + (LAYERS - 1) * CHANNELS * CHANNELS) * N_SITES
 GATHER_FLOP = 2 * N_OCC * N_OCC * D_FEAT
 PFAFFIAN_FLOP = N_OCC ** 3 / 3.0
 FP32_CORE_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FMA rate of the CUDA cores
-# DRAM bytes per launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum), keyed by
-# kernel; filled from the committed summaries under profiles/.  None until captured.
-TRAFFIC_BYTES = {"pfaffian": None, "cnn": None}
+# DRAM bytes per amplitude from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum of a
+# 2048-matrix launch, divided by 2048: traffic grows in proportion to the matrices), keyed by
+# kernel; the figures are those of the summaries under profiles/.
+TRAFFIC_BYTES = {"pfaffian": 31.3e6 / 2048}
 
 
 def peaks():
@@ -162,12 +169,148 @@ def cpu_baseline(target_s: float = 12.0) -> dict:
 
 # ---------------------------------------------------------------- GPU arm
 
+def time_amplitudes(state, spins, steps, warmup, flush, st, profile=False):
+    """Warm-up, then ``steps`` timed calls of ``state(spins)`` with L2 flushed between them
+    (outside the events).  Returns (summed step milliseconds, per-kernel profile or {})."""
+    import torch
+
+    from neuralhubbard_b200 import _lib
+
+    for _ in range(warmup):
+        state(spins)
+    torch.cuda.synchronize()
+    if profile:
+        _lib.profile_read()
+        _lib.profile_enable(True)
+    ev = []
+    for _ in range(steps):
+        flush.fill_(1)  # evict L2 between steps (not timed)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        state(spins)
+        e1.record(st)
+        ev.append((e0, e1))
+    torch.cuda.synchronize()
+    kern = {}
+    if profile:
+        _lib.profile_enable(False)
+        kern = _lib.profile_read()
+    return sum(a.elapsed_time(b) for a, b in ev), kern
+
+
+def run_chains(smp, steps, st):
+    """``steps`` Metropolis steps, one call each, recording log|psi| of every chain; returns
+    (log|psi| series (steps, B) on the host, device milliseconds, acceptance)."""
+    import torch
+
+    B = smp.nsamples
+    series = torch.empty((steps, B), dtype=torch.float64, device=smp.spins.device)
+    a0 = int(smp.accepted.sum().item())
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for t in range(steps):
+        smp.run(1)
+        series[t].copy_(smp.psi.logabs)
+    e1.record(st)
+    torch.cuda.synchronize()
+    acc = (int(smp.accepted.sum().item()) - a0) / (B * steps)
+    return series.cpu().numpy(), e0.elapsed_time(e1), acc
+
+
+def measure_sampling(args, dev, st, seed) -> dict:
+    """Effective samples/s of the plain form (FP32 CNN, uniform-hop sampler) and the chosen form
+    (tcgen05 BF16x3 CNN, learned proposal trained on 2^20 records of plain chains), plus the
+    chosen amplitudes under the uniform-hop sampler.  All chains start from the same
+    configurations, equilibrated by ``burn`` plain steps; tau_int is that of the log|psi| series
+    over the ``steps`` measured steps; energies per site from the final configurations."""
+    import torch
+
+    import neuralhubbard_b200 as nh
+    from neuralhubbard_b200 import stats
+
+    B, steps, burn = args.chains, args.sampler_steps, args.burn
+    params = nh.init_params(L, L, CHANNELS, LAYERS, std=0.02, seed=0)
+    forms = {
+        "plain": nh.PfaffianBackflow(L, L, NE, NE, params=params, device=dev, cnn_mode=0),
+        "chosen": nh.PfaffianBackflow(L, L, NE, NE, params=params, device=dev, cnn_mode=2,
+                                      pf_mode=args.pf_mode),
+    }
+    states = {k: nh.Variational(m, symm=True, max_parallel=8192) for k, m in forms.items()}
+    init = nh.random_spins(np.random.default_rng(seed), B, N_SITES, NE, NE)
+    eq = nh.ParticleHop(states["chosen"], B, n_neighbor=(1, 2), initial_spins=init, seed=seed)
+    n_snap = min(burn, max(1, (1 << 20) // B))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eq.run(burn - n_snap)
+    snaps = []
+    for _ in range(n_snap):  # training records: the chains' last 2^20 / B configurations
+        eq.run(1)
+        snaps.append(eq.spins.clone())
+    torch.cuda.synchronize()
+    t_burn = time.perf_counter() - t0
+    start = eq.spins.clone()
+    t0 = time.perf_counter()
+    rec = nh.training_records(states["chosen"], torch.cat(snaps), seed=seed + 2,
+                              weight="barker")
+    torch.cuda.synchronize()
+    t_rec = time.perf_counter() - t0
+    del snaps
+    q = nh.HopProposal(L, L, 8, seed=seed + 3, std=0.05, device=dev)
+    t0 = time.perf_counter()
+    losses = q.train(rec, args.train_steps, batch=512, lr=3e-3, seed=seed + 4)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    train = {"records": int(rec[0].shape[0]), "steps": args.train_steps, "batch": 512,
+             "target": "barker r/(1+r)", "record_seconds": t_rec, "train_seconds": t_train,
+             "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:]))}
+    del rec
+
+    out = {}
+    H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2])
+    ne = min(B, args.energy_samples)
+    runs = [("plain", "plain", lambda s: nh.ParticleHop(states["plain"], B, n_neighbor=(1, 2),
+                                                        initial_spins=s, seed=seed + 5)),
+            ("chosen", "chosen", lambda s: nh.LearnedHop(states["chosen"], B, q,
+                                                         initial_spins=s, seed=seed + 6)),
+            ("chosen_uniform_hop", "chosen",
+             lambda s: nh.ParticleHop(states["chosen"], B, n_neighbor=(1, 2), initial_spins=s,
+                                      seed=seed + 7))]
+    for name, form, make in runs:
+        smp = make(start)
+        series, ms, acc = run_chains(smp, steps, st)
+        tau = stats.tau_int(series)
+        e = H.Oloc(states[form], nh.Samples(smp.spins[:ne].contiguous(), smp.psi[:ne]))
+        e = e.cpu().numpy() / N_SITES
+        out[name] = {"acceptance": acc, "tau_int_logpsi": tau, "ms_per_step": ms / steps,
+                     "effective_samples_per_s": stats.effective_rate(B, steps, tau, ms / 1e3),
+                     "energy_per_site": float(e.mean()),
+                     "energy_per_site_err": float(e.std(ddof=1) / np.sqrt(ne))}
+        del smp
+    out["chosen"]["proposal_training"] = train
+    d = out["chosen"]["energy_per_site"] - out["plain"]["energy_per_site"]
+    sig = float(np.hypot(out["chosen"]["energy_per_site_err"], out["plain"]["energy_per_site_err"]))
+    out["energy_difference_sigma"] = abs(d) / sig if sig > 0 else None
+    out["chosen_vs_plain"] = (out["chosen"]["effective_samples_per_s"]
+                              / out["plain"]["effective_samples_per_s"])
+    out["chosen_uniform_hop_vs_plain"] = (out["chosen_uniform_hop"]["effective_samples_per_s"]
+                                          / out["plain"]["effective_samples_per_s"])
+    out["setup"] = {"chains": B, "burn_in_steps": burn, "burn_in_seconds": t_burn,
+                    "measured_steps": steps,
+                    "start": "all runs from the same configurations after the burn-in",
+                    "tau_convention": "Sokal tau = 1/2 + sum rho (window c = 5); effective = "
+                                      "B steps / (2 tau seconds)",
+                    "energy_samples": ne, "seconds_are": "CUDA-event time of the measured steps"}
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
 
     import neuralhubbard_b200 as nh
-    from neuralhubbard_b200 import _lib
     from neuralhubbard_b200.distributed import init_from_env
 
     rank = int(os.environ.get("RANK", "0"))
@@ -187,40 +330,37 @@ def run_ours(args) -> None:
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=dev)
     st = torch.cuda.current_stream(dev)
 
-    for _ in range(args.warmup):
-        state(spins)
-    torch.cuda.synchronize(dev)
-
     clocks = ClockSampler(local)
     clocks.start()
     if multi:
         dist.barrier()
-    torch.cuda.synchronize(dev)
-    _lib.profile_read()
-    _lib.profile_enable(True)
-    step_ms = []
-    for _ in range(args.steps):
-        flush.fill_(1)  # evict L2 between steps (not timed)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        psi = state(spins)
-        e1.record(st)
-        step_ms.append((e0, e1))
-    torch.cuda.synchronize(dev)
-    _lib.profile_enable(False)
-    kern = _lib.profile_read()
+    total_ms, kern = time_amplitudes(state, spins, args.steps, args.warmup, flush, st, True)
     if multi:
         dist.barrier()
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
-    total_ms = sum(a.elapsed_time(b) for a, b in step_ms)
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if multi:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_ms = float(t.item())
     n_amp = world * BATCH * IMAGES * args.steps
     value = n_amp / (total_ms / 1e3)
+
+    # the plain FP32 form on the same inputs (reported beside the chosen form)
+    plain = None
+    if args.cnn_mode != 0 or args.pf_mode != 0:
+        m0 = nh.PfaffianBackflow(L, L, NE, NE, params=params, device=dev, cnn_mode=0)
+        s0 = nh.Variational(m0, symm=True, max_parallel=BATCH)
+        p_ms, p_kern = time_amplitudes(s0, spins, args.steps, args.warmup, flush, st, True)
+        tp = torch.tensor([p_ms], dtype=torch.float64, device=dev)
+        if multi:
+            dist.all_reduce(tp, op=dist.ReduceOp.MAX)
+        p_ms = float(tp.item())
+        plain = {"value": n_amp / (p_ms / 1e3), "ms_per_step": p_ms / args.steps,
+                 "form": "FP32 CUDA-core CNN, CUDA-core Pfaffian",
+                 "kernels": {k: {"ms_per_step": v[0] / args.steps, "launches": v[1]}
+                             for k, v in p_kern.items()}}
+        del m0, s0
 
     # e2e: public API, configurations from pinned host memory, amplitudes back to the host
     sign_h = torch.empty(BATCH, dtype=torch.float32).pin_memory()
@@ -257,13 +397,19 @@ def run_ours(args) -> None:
         achieved = flop * amps_per_launch / per_launch_s / 1e12
         tb = TRAFFIC_BYTES.get(dom)
         roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": bf16,
-                "unit": "TFLOP/s", "frac": achieved / bf16, "traffic": tb,
+                "unit": "TFLOP/s", "frac": achieved / bf16,
+                "traffic": tb * amps_per_launch if tb else None,
                 "peak_source": f"{peak_kind} bf16 dense (MEASURED_PEAKS.json)",
                 "fp32_core_frac": achieved / FP32_CORE_PEAK_TFLOPS,
-                "note": "FP32 CUDA-core kernel; fp32_core_frac is against the nominal FP32 FMA "
-                        "rate of 148 SMs at 1965 MHz"}
+                "note": "gather + Pfaffian FLOP (2 n^2 d + n^3 / 3 per amplitude); "
+                        "fp32_core_frac is against the nominal FP32 FMA rate of 148 SMs at "
+                        "1965 MHz, the roof of the CUDA-core kernel"}
     launches = sum(n for _, n in kern.values())
     kernels = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1]} for k, v in kern.items()}
+
+    sampling = None
+    if world == 1 and not args.no_sampling:
+        sampling = measure_sampling(args, dev, st, seed=77)
 
     if rank == 0:
         cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
@@ -283,8 +429,10 @@ def run_ours(args) -> None:
                        "cnn": "4 x periodic 3x3, 32 channels, tanh-GELU, N(0, 0.02)",
                        "l2": "512 MiB written between timed steps, outside the step events",
                        "parallelism": f"replicas x{world} (chains data-parallel)"},
+            "plain": plain,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": BATCH * 2 * N_SITES,
                     "d2h_bytes_per_step": BATCH * (4 + 8)},
+            "sampling": sampling,
             "roofline": roof, "kernels": kernels, "gpu_launches": launches,
             "cpu_baseline": cpu, "clocks": clk,
         }
@@ -329,10 +477,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cnn-mode", type=int, default=0, choices=[0, 1, 2],
+    ap.add_argument("--cnn-mode", type=int, default=2, choices=[0, 1, 2],
                     help="0: FP32 CUDA-core CNN (plain form); 1: tcgen05 BF16; 2: tcgen05 BF16x3")
     ap.add_argument("--pf-mode", type=int, default=0, choices=[0, 1],
                     help="0: CUDA-core Pfaffian; 1: matrix in tensor memory, tcgen05 updates")
+    ap.add_argument("--no-sampling", action="store_true",
+                    help="skip the effective-samples comparison of the two sampler forms")
+    ap.add_argument("--chains", type=int, default=1024)
+    ap.add_argument("--sampler-steps", type=int, default=2000)
+    ap.add_argument("--burn", type=int, default=6000)
+    ap.add_argument("--train-steps", type=int, default=2000)
+    ap.add_argument("--energy-samples", type=int, default=512)
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="configurations per step (default 8192; smaller only for profiling)")
     args = ap.parse_args()

@@ -564,14 +564,17 @@ __global__ void __launch_bounds__(1024) flagged_kernel(const int32_t* __restrict
 // columns [0, NP), rows 128-255 in columns [NP, 2 NP), NP = n rounded up to 32); thread t owns
 // row t and reads pivot columns with tcgen05.ld.  The panel is the same relabelling Parlett-Reid
 // as pfaffian_kernel; at the end of each panel of 8 steps the rank-16 update
-// A += U V^T - V U^T runs on the tensor cores as 3xTF32 products (X = X_big + X_small):
-// U_b V_b^T + U_b V_s^T + U_s V_b^T - V_b U_b^T - V_b U_s^T - V_s U_b^T, six kind::tf32 MMAs
-// (M = 128, N = NP, K = 8) per 128-row tile, the minus signs via the A-negate bit of the
-// instruction descriptor.  Rows and columns of eliminated indices carry U = V = 0 and never
+// A += U V^T - V U^T runs on the tensor cores as 3xTF32 products (X = X_big + X_small, both
+// rounded to TF32): U_b V_b^T + U_b V_s^T + U_s V_b^T - V_b U_b^T - V_b U_s^T - V_s U_b^T, six
+// kind::tf32 MMAs (M = 128, N = NP, K = 8) per 128-row tile, the minus signs via the A-negate bit
+// of the instruction descriptor.  Accuracy: the accumulation into the FP32 matrix in tensor
+// memory, not the operand split, limits this form (a three-way split measured no better); at
+// n = 224 log|pf| is within about 2e-4 of FP64, against 1e-4 for the CUDA-core kernel.  Rows and columns of eliminated indices carry U = V = 0 and never
 // change again.  The occupied block is gathered into a shared-memory lower triangle first and
 // copied into tensor memory with tcgen05.st.
 
 constexpr int kTcNB = 8;
+constexpr int kTcOpFloats = 4 * 2048 + 2 * kNumThreads * kTcNB;  // operands + FP32 panel copies
 constexpr uint32_t kTcCols = 512;
 constexpr long long kTcWaitLimit = 1ll << 22;
 
@@ -661,7 +664,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, i
   const int NP = (n + 31) & ~31;
   const int n_tiles = (n + 127) >> 7;
   float* region = reinterpret_cast<float*>(smem_raw);  // staging triangle, later the operands
-  const int region_floats = max((tri + 31) & ~31, 4 * 2048 + 2 * kNumThreads * kTcNB);
+  const int region_floats = max((tri + 31) & ~31, kTcOpFloats);
   float* Ub = region;               // 4 operand arrays of 256 x 8 TF32 (8 KB each)
   float* Us = region + 2048;
   float* Vb = region + 4096;
@@ -751,10 +754,8 @@ __global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, i
         myU[j] = 0.0f;
         myV[j] = 0.0f;
         if (j >= steps) {  // columns a short last panel leaves unused must be zero
-          Ub[opnd_off(tid, j)] = 0.0f;
-          Us[opnd_off(tid, j)] = 0.0f;
-          Vb[opnd_off(tid, j)] = 0.0f;
-          Vs[opnd_off(tid, j)] = 0.0f;
+          const int o = opnd_off(tid, j);
+          Ub[o] = Us[o] = Vb[o] = Vs[o] = 0.0f;
         }
       }
 #pragma unroll
@@ -817,11 +818,12 @@ __global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, i
             Vf[tid * kTcNB + j] = v;
             // Both parts rounded to TF32 here: the tensor cores would truncate an unrounded
             // small part, a bias that accumulates over the pivots.
+            const int o = opnd_off(tid, j);
             const float ub = tf32_big(u), vb = tf32_big(v);
-            Ub[opnd_off(tid, j)] = ub;
-            Us[opnd_off(tid, j)] = tf32_big(u - ub);
-            Vb[opnd_off(tid, j)] = vb;
-            Vs[opnd_off(tid, j)] = tf32_big(v - vb);
+            Ub[o] = ub;
+            Us[o] = tf32_big(u - ub);
+            Vb[o] = vb;
+            Vs[o] = tf32_big(v - vb);
             if (my_log == k + 2) misc[0] = tid;
             if (tid == 0) pivs[k >> 1] = lr != k + 1 ? -piv : piv;
           }
@@ -836,19 +838,23 @@ __global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, i
       __syncthreads();
       if (tid == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t ub = smem_addr(Ub), us = smem_addr(Us), vb = smem_addr(Vb),
-                       vs = smem_addr(Vs);
+        // Products of the parts: big x big, big x small, small x big.
+        const uint32_t u2[2] = {smem_addr(Ub), smem_addr(Us)};
+        const uint32_t v2[2] = {smem_addr(Vb), smem_addr(Vs)};
+        constexpr int kPa[3] = {0, 0, 1}, kPb[3] = {0, 1, 0};
         const uint32_t lbo = 4096, sbo = 128;
         const uint32_t id_pos = tf32_idesc(NP, false), id_neg = tf32_idesc(NP, true);
         for (int mt = 0; mt < n_tiles; ++mt) {
           const uint32_t d = tmem + (uint32_t)(mt * NP);
           const uint32_t ro = (uint32_t)(mt * 128 / 8 * 128);  // first row group of the tile
-          mma_tf32(d, tc_desc(ub + ro, lbo, sbo), tc_desc(vb, lbo, sbo), id_pos);
-          mma_tf32(d, tc_desc(ub + ro, lbo, sbo), tc_desc(vs, lbo, sbo), id_pos);
-          mma_tf32(d, tc_desc(us + ro, lbo, sbo), tc_desc(vb, lbo, sbo), id_pos);
-          mma_tf32(d, tc_desc(vb + ro, lbo, sbo), tc_desc(ub, lbo, sbo), id_neg);
-          mma_tf32(d, tc_desc(vb + ro, lbo, sbo), tc_desc(us, lbo, sbo), id_neg);
-          mma_tf32(d, tc_desc(vs + ro, lbo, sbo), tc_desc(ub, lbo, sbo), id_neg);
+#pragma unroll
+          for (int t = 0; t < 3; ++t) {  // + U V^T
+            mma_tf32(d, tc_desc(u2[kPa[t]] + ro, lbo, sbo), tc_desc(v2[kPb[t]], lbo, sbo), id_pos);
+          }
+#pragma unroll
+          for (int t = 0; t < 3; ++t) {  // - V U^T
+            mma_tf32(d, tc_desc(v2[kPa[t]] + ro, lbo, sbo), tc_desc(u2[kPb[t]], lbo, sbo), id_neg);
+          }
         }
         asm volatile(
             "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -911,8 +917,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, i
 
 size_t pf_tc_smem(int n) {
   const size_t tri = (size_t)n * (n - 1) / 2;
-  const size_t region = std::max((tri + 31) & ~(size_t)31,
-                                 (size_t)(4 * 2048 + 2 * kNumThreads * kTcNB));
+  const size_t region = std::max((tri + 31) & ~(size_t)31, (size_t)kTcOpFloats);
   const size_t need = sizeof(float) * (region + 128 + kWarps) + sizeof(int) * (2 * kWarps + 4) + 32;
   // At least 120 KB, so that two CTAs never share an SM: each allocates all 512 tensor-memory
   // columns, and a second CTA would stall in tcgen05.alloc until the first one exits.
@@ -922,13 +927,11 @@ size_t pf_tc_smem(int n) {
 template <int D>
 int launch_pf_tc(const PfArgs& a, int32_t* err, cudaStream_t st) {
   const size_t smem = pf_tc_smem(a.n);
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(pfaffian_tc_kernel<D>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "tensor-memory Pfaffian smem attribute");
-    configured = true;
-  }
+  // The limit is raised once, to the largest size any n <= 256 needs.
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      pfaffian_tc_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)pf_tc_smem(kNumThreads));
+  if (attr != cudaSuccess) return check_cuda(attr, "tensor-memory Pfaffian smem attribute");
   int grid = num_sms();
   if (grid > a.n_slots) grid = a.n_slots;
   if (grid <= 0) return NH_OK;

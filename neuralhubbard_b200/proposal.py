@@ -7,9 +7,9 @@ own forward/backward/Adam kernels, and it is used under an exact Metropolis-Hast
 so the sampled distribution stays |psi|^2 whatever the network has learned.
 
 Training data: configurations taken from plain-sampler chains; for each, one move drawn
-uniformly among its valid moves and the weight w = min(1, |psi(s')/psi(s)|^2).  The loss
--(1/B) sum w log q(m | s) is minimised by a proposal that offers moves in proportion to their
-Metropolis acceptance.
+uniformly among its valid moves and a weight w(|psi(s')/psi(s)|^2) (``target_weight``: the
+Metropolis acceptance min(1, r) by default, or a locally balanced sqrt(r) or r / (1 + r)).  The
+loss -(1/B) sum w log q(m | s) is minimised by a proposal that offers moves in proportion to w.
 """
 
 from __future__ import annotations
@@ -171,10 +171,28 @@ def apply_moves(spins: torch.Tensor, moves: torch.Tensor, Lx: int, Ly: int) -> t
     return out
 
 
+WEIGHTS = ("acceptance", "sqrt", "barker")
+
+
+def target_weight(lr2: torch.Tensor, kind: str, clip: float = 20.0) -> torch.Tensor:
+    """Training weight of a move with log |psi(s')/psi(s)|^2 = lr2.  The loss is minimised by
+    q(m | s) proportional to the weight: "acceptance" min(1, r), or the locally balanced
+    proposals of G. Zanella, JASA 115 (2020) 852, "sqrt" sqrt(r) (clipped) and "barker"
+    r / (1 + r)."""
+    if kind == "acceptance":
+        return torch.exp(torch.clamp(lr2, max=0.0))
+    if kind == "sqrt":
+        return torch.exp(torch.clamp(0.5 * lr2, max=float(np.log(clip))))
+    if kind == "barker":
+        return torch.sigmoid(lr2)
+    raise ValueError(f"weight {kind!r} not in {WEIGHTS}")
+
+
 def training_records(state: Variational, spins, psi: Optional[LogArray] = None, seed: int = 0,
-                     n_dirs: int = 8, chunk: int = 65536):
-    """(spins, moves, weights) records: one uniformly drawn valid move per configuration and
-    w = min(1, |psi(s')/psi(s)|^2), with the amplitudes from ``state`` (one per record)."""
+                     n_dirs: int = 8, chunk: int = 65536, weight: str = "acceptance"):
+    """(spins, moves, weights) records: one uniformly drawn valid move per configuration and its
+    ``target_weight`` (default min(1, |psi(s')/psi(s)|^2)), with the amplitudes from ``state``
+    (one evaluation per record)."""
     g = state.model.geom
     spins = as_spins(spins, state.device)
     B = spins.shape[0]
@@ -192,7 +210,7 @@ def training_records(state: Variational, spins, psi: Optional[LogArray] = None, 
         sp = apply_moves(s, m, g.LX, g.LY)
         phi = state(sp)
         lr2 = 2.0 * (phi.logabs - psi.logabs[a : a + chunk])
-        w = torch.exp(torch.clamp(lr2, max=0.0)).to(torch.float32)
+        w = target_weight(lr2, weight).to(torch.float32)
         w = torch.where((phi.sign != 0) & ok.any(1), w, torch.zeros_like(w))
         moves[a : a + chunk] = m
         weights[a : a + chunk] = w

@@ -98,3 +98,24 @@ def test_energy_stats_gloo_two_ranks():
         assert n == 1000
         assert m == pytest.approx(e_all.mean(), abs=1e-12)
         assert v == pytest.approx(e_all.var(), rel=1e-9)
+
+
+def test_tau_int_matches_oracle_and_ar1():
+    """The package's chain statistics against the oracle's and the AR(1) closed form
+    tau = (1 + phi) / (2 (1 - phi))."""
+    from neuralhubbard_b200 import stats
+    from oracle import sampler as osam
+
+    rng = np.random.default_rng(0)
+    phi, T, B = 0.8, 4000, 64
+    x = np.zeros((T, B))
+    e = rng.normal(size=(T, B))
+    for t in range(1, T):
+        x[t] = phi * x[t - 1] + e[t]
+    tau = stats.tau_int(x)
+    assert abs(tau - osam.tau_int(x)) < 1e-12
+    assert abs(tau - (1 + phi) / (2 * (1 - phi))) < 0.25
+    m, err = stats.jackknife_mean(x[:, 0])
+    m0, err0 = osam.jackknife_mean(x[:, 0])
+    assert m == m0 and abs(err - err0) < 1e-12
+    assert stats.effective_rate(64, 4000, 0.5, 2.0) == 64 * 4000 / 2.0
