@@ -15,7 +15,8 @@ amplitudes read back every step.
 chosen form (tcgen05 BF16x3 CNN, learned hop proposal with the exact Hastings correction,
 trained on 2^20 records of the plain chains): acceptance, tau_int of the log|psi| series,
 effective samples per second and the energy per site of each, on 1024 chains that start from
-the same configurations after 6000 equilibration steps.
+the same configurations after 6000 equilibration steps.  ``local_energy`` (1 GPU) times the
+ragged local energy of 4096 configurations at 8x8 and 16x16, one CUDA-graph replay each.
 
 Under torchrun each rank evaluates its own 8192 configurations (weak scaling); the time is the
 maximum over ranks of the summed per-step CUDA-event durations.  ``--impl reference`` times the
@@ -306,6 +307,65 @@ def measure_sampling(args, dev, st, seed) -> dict:
     return out
 
 
+def measure_local_energy(args, dev, st) -> dict:
+    """Ragged local energy (unprojected amplitudes, CUDA-core Pfaffian; FP32 CNN, and at 16x16
+    also the tcgen05 BF16x3 CNN) of ``eloc_samples`` configurations per lattice: the chunk size
+    is tuned on 256 of them, then one call is recorded in a CUDA graph and its replay timed with
+    CUDA events."""
+    import torch
+
+    import neuralhubbard_b200 as nh
+
+    out = {}
+    H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2])
+    for Lk, cnn_mode in ((8, 0), (16, 0), (16, 2)):
+        Nk = Lk * Lk
+        nek = 7 * Nk // 16
+        params = nh.init_params(Lk, Lk, CHANNELS, LAYERS, std=0.02, seed=0)
+        model = nh.PfaffianBackflow(Lk, Lk, nek, nek, params=params, device=dev,
+                                    cnn_mode=cnn_mode)
+        state = nh.Variational(model, symm=False, max_parallel=8192)
+        B = args.eloc_samples
+        spins = torch.from_numpy(nh.random_spins(np.random.default_rng(500 + Lk), B, Nk, nek,
+                                                 nek)).to(dev)
+        psi = state(spins)
+        sub = nh.Samples(spins[:256].contiguous(), psi[:256])
+        chunk = H.autotune(state, sub, candidates=(4096, 16384, 65536), repeats=1)
+        counts = H.hop_list(spins, Lk, Lk)[0]
+        n_conn = int(counts.sum().item())
+        samples = nh.Samples(spins, psi)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            H.Oloc(state, nh.Samples(spins[:64].contiguous(), psi[:64]), chunk_configs=chunk,
+                   count_connections=False)
+        torch.cuda.current_stream().wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            e = H.Oloc(state, samples, chunk_configs=chunk, count_connections=False)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        graph.replay()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        ev = e.cpu().numpy() / Nk
+        out[f"{Lk}x{Lk}" + ("" if cnn_mode == 0 else " tcgen05 BF16x3 CNN")] = {
+            "samples": B, "connections": n_conn, "pfaffian_n": 2 * nek, "chunk_configs": chunk,
+            "ms": ms, "samples_per_s": B / (ms / 1e3),
+            "amplitudes_per_s": n_conn / (ms / 1e3),
+            "energy_per_site": float(ev.mean()),
+            "energy_per_site_err": float(ev.std(ddof=1) / np.sqrt(B))}
+        del graph, e, state, model
+        torch.cuda.empty_cache()
+    out["setup"] = ("4096 uniformly random configurations per lattice, unprojected amplitudes, "
+                    "t = 1, t' = -0.2, U = 8; one CUDA-graph replay of the whole call; "
+                    "24x24 (n = 504) exceeds the shared-memory Pfaffian (n <= 256)")
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -410,6 +470,9 @@ def run_ours(args) -> None:
     sampling = None
     if world == 1 and not args.no_sampling:
         sampling = measure_sampling(args, dev, st, seed=77)
+    local_energy = None
+    if world == 1 and not args.no_eloc:
+        local_energy = measure_local_energy(args, dev, st)
 
     if rank == 0:
         cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
@@ -433,6 +496,7 @@ def run_ours(args) -> None:
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": BATCH * 2 * N_SITES,
                     "d2h_bytes_per_step": BATCH * (4 + 8)},
             "sampling": sampling,
+            "local_energy": local_energy,
             "roofline": roof, "kernels": kernels, "gpu_launches": launches,
             "cpu_baseline": cpu, "clocks": clk,
         }
@@ -483,6 +547,9 @@ def main():
                     help="0: CUDA-core Pfaffian; 1: matrix in tensor memory, tcgen05 updates")
     ap.add_argument("--no-sampling", action="store_true",
                     help="skip the effective-samples comparison of the two sampler forms")
+    ap.add_argument("--no-eloc", action="store_true",
+                    help="skip the ragged local-energy measurement (8x8 and 16x16)")
+    ap.add_argument("--eloc-samples", type=int, default=4096)
     ap.add_argument("--chains", type=int, default=1024)
     ap.add_argument("--sampler-steps", type=int, default=2000)
     ap.add_argument("--burn", type=int, default=6000)

@@ -178,8 +178,12 @@ int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_p
                  size_t workspace_bytes, void* stream);
 
 /* Local energies E_loc (batch,) FP64 of configurations with amplitudes (sign, logabs).  The
- * connected configurations are evaluated in chunks of at most chunk_configs configurations
- * (0 = default).  Synchronises the stream once to read the number of connections. */
+ * ragged list of connected configurations is evaluated in chunks of chunk_configs
+ * configurations (0 = default) whose work counts stay on the device.  With n_conn_out null the
+ * call never synchronises: its launch sequence depends only on the arguments (batch x
+ * electrons x 8 / chunk chunks; the empty ones return at once), so a caller may record it into
+ * a CUDA graph and replay it.  With n_conn_out set it synchronises the stream once, writes the
+ * number of connections and launches only the chunks that hold connections. */
 size_t nh_local_energy_workspace_bytes(int batch, int n_symm, int chunk_configs,
                                        const nh_backflow_params* p);
 int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs, int batch,

@@ -328,6 +328,8 @@ struct ElocLayout {
   int32_t* to;
   float* csign;
   double* clogabs;
+  int32_t* chunk_cnt;  // device work count of every chunk of the connection list
+  int n_chunks;
   void* pipe;
   size_t bytes;
 };
@@ -352,6 +354,8 @@ static ElocLayout eloc_layout(void* ws, int batch, int n_symm, int chunk,
   L.to = reinterpret_cast<int32_t*>(take(cmax * 4));
   L.csign = reinterpret_cast<float*>(take(cmax * 4));
   L.clogabs = reinterpret_cast<double*>(take(cmax * 8));
+  L.n_chunks = (int)((cmax + chunk - 1) / chunk);
+  L.chunk_cnt = reinterpret_cast<int32_t*>(take((size_t)L.n_chunks * 4));
   L.pipe = take(pipeline_bytes(chunk * n_symm, n, d));
   L.bytes = off;
   return L;
@@ -384,24 +388,33 @@ int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs
   const int N = p->Lx * p->Ly, n = p->n_up + p->n_dn, d = p->channels / 2;
   if ((rc = launch_hop_count(spins, batch, p->Lx, p->Ly, h->n_dirs, L.counts, st))) return rc;
   if ((rc = launch_scan_counts(L.counts, batch, L.offsets, st))) return rc;
+  // At most n_dirs hops per electron: the emitted list never exceeds cmax (the emit kernel
+  // also stops at cmax).
   const int64_t cmax = (int64_t)batch * n * 8;
   if ((rc = launch_hop_emit(spins, batch, p->Lx, p->Ly, *h, L.offsets, cmax, nullptr, L.hval,
                             L.owner, L.from, L.to, st)))
     return rc;
-  int64_t total = 0;
-  if ((rc = check_cuda(cudaMemcpyAsync(&total, L.offsets + batch, sizeof(int64_t),
-                                       cudaMemcpyDeviceToHost, st),
-                       "local_energy: read connection count")))
+  // The ragged connection list is processed in chunks whose work counts live on the device, so
+  // the launch sequence does not depend on the data.  Without n_conn_out the call never waits
+  // for the GPU and runs all ceil(cmax / chunk) chunks (the empty ones exit at once); with it,
+  // the count is read back first and only the chunks that hold connections are launched.
+  if ((rc = launch_chunk_counts(L.offsets + batch, L.n_chunks, chunk, L.chunk_cnt, st)))
     return rc;
-  if ((rc = check_cuda(cudaStreamSynchronize(st), "local_energy: sync"))) return rc;
-  if (n_conn_out) *n_conn_out = total;
-  if (total > cmax)
-    return fail(NH_ERR_INVALID, "local_energy: %lld connections exceed %lld (more than %d "
-                "electrons in a configuration)", (long long)total, (long long)cmax, n);
+  int used = L.n_chunks;
+  if (n_conn_out) {
+    int64_t total = 0;
+    if ((rc = check_cuda(cudaMemcpyAsync(&total, L.offsets + batch, sizeof(int64_t),
+                                         cudaMemcpyDeviceToHost, st),
+                         "local_energy: read connection count")))
+      return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(st), "local_energy: sync"))) return rc;
+    *n_conn_out = total;
+    used = (int)((total + chunk - 1) / chunk);
+  }
   PipelineBuffers b = carve_pipeline(L.pipe, chunk * n_symm, n, d);
-  for (int64_t c0 = 0; c0 < total; c0 += chunk) {
-    const int nc = (int)((total - c0) < chunk ? (total - c0) : chunk);
-    ConfigList cl{spins, L.owner + c0, L.from + c0, L.to + c0, nullptr, nc, n_symm};
+  for (int i = 0; i < used; ++i) {
+    const int64_t c0 = (int64_t)i * chunk;
+    ConfigList cl{spins, L.owner + c0, L.from + c0, L.to + c0, L.chunk_cnt + i, chunk, n_symm};
     if ((rc = run_pipeline(cl, *p, b, L.csign + c0, L.clogabs + c0, nullptr, st))) return rc;
   }
   return launch_eloc_reduce(spins, sign, logabs, batch, N, h->U, L.offsets, L.hval, L.csign,

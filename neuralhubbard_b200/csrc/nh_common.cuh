@@ -214,6 +214,8 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
 int launch_hop_count(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs,
                      int32_t* counts, cudaStream_t st);
 int launch_scan_counts(const int32_t* counts, int batch, int64_t* offsets, cudaStream_t st);
+int launch_chunk_counts(const int64_t* total, int n_chunks, int chunk, int32_t* out,
+                        cudaStream_t st);
 // Writes at most cap records (connections beyond cap, only possible for configurations with
 // more electrons than the buffers were sized for, are dropped; callers check the total).
 int launch_hop_emit(const int8_t* spins, int batch, int Lx, int Ly, const nh_hubbard_params& h,

@@ -359,6 +359,25 @@ int launch_hop_count(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs,
   return check_launch("hop_kernel<count>");
 }
 
+// Work count of every chunk of the connection list: clamp(total - i * chunk, 0, chunk), with
+// total = offsets[batch] read on the device (no host round trip).
+__global__ void chunk_counts_kernel(const int64_t* __restrict__ total, int n_chunks, int chunk,
+                                    int32_t* __restrict__ out) {
+  const int64_t t = *total;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_chunks; i += gridDim.x * blockDim.x) {
+    const int64_t left = t - (int64_t)i * chunk;
+    out[i] = (int32_t)(left <= 0 ? 0 : (left < chunk ? left : chunk));
+  }
+}
+
+int launch_chunk_counts(const int64_t* total, int n_chunks, int chunk, int32_t* out,
+                        cudaStream_t st) {
+  if (n_chunks <= 0) return NH_OK;
+  ProfScope prof_scope(NH_K_SCAN, st);
+  chunk_counts_kernel<<<(n_chunks + 255) / 256, 256, 0, st>>>(total, n_chunks, chunk, out);
+  return check_launch("chunk_counts_kernel");
+}
+
 int launch_scan_counts(const int32_t* counts, int batch, int64_t* offsets, cudaStream_t st) {
   ProfScope prof_scope(NH_K_SCAN, st);
   scan_kernel<<<1, 1024, 0, st>>>(counts, batch, offsets);

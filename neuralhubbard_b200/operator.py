@@ -5,13 +5,25 @@ Samples(spins, psi))`` call of ``code/quick_start.py:33``; H built as
 from __future__ import annotations
 
 import ctypes
-from typing import Sequence, Union
+import threading
+from typing import Dict, Optional, Sequence, Tuple, Union
 
 import torch
 
 from . import _lib
 from .backflow import stream_ptr, workspace
 from .state import Samples, Variational, as_spins
+
+
+_CHUNK_LOCK = threading.Lock()
+_CHUNK_CACHE: Dict[Tuple, int] = {}
+
+
+def _tune_key(state: Variational, H: "Hubbard") -> Tuple:
+    g = state.model.geom
+    m = state.model
+    return (str(state.device), g.LX, g.LY, g.n_up, g.n_dn, state.n_symm, H.n_dirs,
+            getattr(m, "cnn_mode", 0), getattr(m, "pf_mode", 0))
 
 
 class Hubbard:
@@ -29,16 +41,24 @@ class Hubbard:
         self.t = ts[0]
         self.tp = ts[1] if len(ts) > 1 else 0.0
         self.n_dirs = 8 if len(ts) > 1 else 4
-        self.last_n_conn = 0
+        self.last_n_conn: Optional[int] = 0
 
     def c_params(self) -> _lib.HubbardParams:
         return _lib.HubbardParams(self.t, self.tp, self.U, self.n_dirs)
 
-    def Oloc(self, state: Variational, samples: Samples, chunk_configs: int = 0) -> torch.Tensor:
-        """(B,) FP64 local energies E_loc(s) = sum_s' <s|H|s'> psi(s') / psi(s)."""
+    def Oloc(self, state: Variational, samples: Samples, chunk_configs: int = 0,
+             count_connections: bool = True) -> torch.Tensor:
+        """(B,) FP64 local energies E_loc(s) = sum_s' <s|H|s'> psi(s') / psi(s).
+
+        ``chunk_configs`` = 0 takes the size ``autotune`` picked for this lattice and form (the
+        library default if none).  With ``count_connections`` the call waits once for the number
+        of connections (kept in ``last_n_conn``) and launches only the chunks that hold some;
+        without it, it never waits for the GPU and can be captured in a CUDA graph."""
         spins = as_spins(samples.spins, state.device)
         psi = samples.psi if samples.psi is not None else state(spins)
         B = spins.shape[0]
+        if chunk_configs <= 0:
+            chunk_configs = _CHUNK_CACHE.get(_tune_key(state, self), 0)
         eloc = torch.empty(B, dtype=torch.float64, device=state.device)
         p = state.model.c_params()
         h = self.c_params()
@@ -48,10 +68,34 @@ class Hubbard:
         nconn = ctypes.c_int64(0)
         _lib.call("nh_local_energy", spins.data_ptr(), psi.sign.contiguous().data_ptr(),
                   psi.logabs.contiguous().data_ptr(), B, state.n_symm, ctypes.byref(p),
-                  ctypes.byref(h), chunk_configs, eloc.data_ptr(), ctypes.byref(nconn),
+                  ctypes.byref(h), chunk_configs, eloc.data_ptr(),
+                  ctypes.byref(nconn) if count_connections else None,
                   ws.data_ptr(), ws.numel(), stream_ptr(state.device))
-        self.last_n_conn = int(nconn.value)
+        self.last_n_conn = int(nconn.value) if count_connections else None
         return eloc
+
+    def autotune(self, state: Variational, samples: Samples,
+                 candidates: Sequence[int] = (2048, 8192, 32768), repeats: int = 2) -> int:
+        """Time ``Oloc`` on ``samples`` for each chunk size (CUDA events, after one warm-up
+        call each), remember the fastest for this lattice, symmetry and precision form, and
+        return it.  Later ``Oloc`` calls with ``chunk_configs`` = 0 use it."""
+        best, best_ms = 0, float("inf")
+        st = torch.cuda.current_stream(state.device)
+        for c in candidates:
+            self.Oloc(state, samples, chunk_configs=int(c))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(repeats):
+                self.Oloc(state, samples, chunk_configs=int(c), count_connections=False)
+            e1.record(st)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / repeats
+            if ms < best_ms:
+                best, best_ms = int(c), ms
+        with _CHUNK_LOCK:
+            _CHUNK_CACHE[_tune_key(state, self)] = best
+        return best
 
     def hop_list(self, spins: torch.Tensor, Lx: int, Ly: int):
         """Connection bookkeeping: (counts (B,), offsets (B+1,), rec (C, 2), hval (C,))."""

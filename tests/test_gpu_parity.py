@@ -367,3 +367,55 @@ def test_metropolis_bookkeeping_replay():
     # particle numbers conserved
     assert np.all((s_gpu[:, : g.N] > 0).sum(1) == g.n_up)
     assert np.all((s_gpu[:, g.N :] > 0).sum(1) == g.n_dn)
+
+
+@pytest.mark.parametrize("symm", [False, True])
+def test_local_energy_in_cuda_graph(symm):
+    """Without the connection count the local energy never waits for the GPU: recorded once in
+    a CUDA graph it replays on new configurations and equals the direct call bit for bit."""
+    L = 8
+    model = make_model(L, std=0.3, seed=12)
+    g = model.geom
+    state = nh.Variational(model, symm=symm)
+    H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2])
+    rng = np.random.default_rng(70)
+    s1 = torch.from_numpy(olat.random_configs(rng, 24, g.N, g.n_up, g.n_dn)).to(DEV)
+    s2 = torch.from_numpy(olat.random_configs(rng, 24, g.N, g.n_up, g.n_dn)).to(DEV)
+    ref = [H.Oloc(state, nh.Samples(s, state(s)), chunk_configs=512) for s in (s1, s2)]
+    assert H.last_n_conn > 0
+    spins = s1.clone()
+    psi = state(spins)
+    sign, logabs = psi.sign.clone(), psi.logabs.clone()
+    samples = nh.Samples(spins, nh.LogArray(sign, logabs))
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):  # warm-up off the capture: workspace and kernel attributes
+        H.Oloc(state, samples, chunk_configs=512, count_connections=False)
+    torch.cuda.current_stream().wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        out = H.Oloc(state, samples, chunk_configs=512, count_connections=False)
+    assert H.last_n_conn is None
+    for s, e_ref in zip((s1, s2), ref):
+        p = state(s)
+        spins.copy_(s)
+        sign.copy_(p.sign)
+        logabs.copy_(p.logabs)
+        graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(out, e_ref)
+
+
+def test_local_energy_chunk_autotune():
+    L = 8
+    model = make_model(L, std=0.3, seed=13)
+    g = model.geom
+    state = nh.Variational(model, symm=False)
+    H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2])
+    s = olat.random_configs(np.random.default_rng(71), 64, g.N, g.n_up, g.n_dn)
+    smp = nh.Samples(torch.from_numpy(s).to(DEV))
+    ref = H.Oloc(state, smp, chunk_configs=4096)
+    best = H.autotune(state, smp, candidates=(1024, 4096, 16384), repeats=1)
+    assert best in (1024, 4096, 16384)
+    e = H.Oloc(state, smp)  # uses the tuned chunk
+    assert torch.allclose(e, ref, rtol=1e-12, atol=0)
