@@ -17,6 +17,8 @@ trained on 2^20 records of the plain chains): acceptance, tau_int of the log|psi
 effective samples per second and the energy per site of each, on 1024 chains that start from
 the same configurations after 6000 equilibration steps.  ``local_energy`` (1 GPU) times the
 ragged local energy of 4096 configurations at 8x8 and 16x16, one CUDA-graph replay each.
+``precision`` (1 GPU) reports each precision form's |delta log|psi_P|| and sign mismatches
+against the library's all-FP64 path, and near-nodal log-Pfaffians at the slogpf boundary.
 
 Under torchrun each rank evaluates its own 8192 configurations (weak scaling); the time is the
 maximum over ranks of the summed per-step CUDA-event durations.  ``--impl reference`` times the
@@ -366,6 +368,87 @@ def measure_local_energy(args, dev, st) -> dict:
     return out
 
 
+def _err_stats(la, l0, sg, s0) -> dict:
+    e = np.abs(la - l0)
+    return {"max": float(e.max()), "p99.9": float(np.quantile(e, 0.999)),
+            "p99": float(np.quantile(e, 0.99)), "mean": float(e.mean()),
+            "count_above_1e-4": int((e > 1e-4).sum()), "sign_mismatches": int((sg != s0).sum())}
+
+
+def measure_precision(dev, st, spins, flush) -> dict:
+    """Config 3: |delta log|psi_P|| and sign mismatches against the all-FP64 path for each
+    precision form on the benchmark's 8192 configurations (projected), with each form's step
+    time; and the log-Pfaffian of 8192 FP32 matrices of 224 x 224, 1% of them near-nodal (one
+    pivot 1e-6 of the others), against FP64 factorisation of the same matrices."""
+    import torch
+
+    import neuralhubbard_b200 as nh
+
+    params = nh.init_params(L, L, CHANNELS, LAYERS, std=0.02, seed=0)
+    forms = [("all FP64 (cond_tau 1, reference)", dict(cnn_mode=0, cond_tau=1.0)),
+             ("plain: FP32 CNN, FP64 recompute of pivot ratio > 100", dict(cnn_mode=0)),
+             ("chosen: tcgen05 BF16x3 CNN, FP64 recompute of pivot ratio > 100",
+              dict(cnn_mode=2)),
+             ("plain + FP64 recompute of configurations cancelling > 8x",
+              dict(cnn_mode=0, cancel_tau=8.0)),
+             ("chosen + FP64 recompute of configurations cancelling > 8x",
+              dict(cnn_mode=2, cancel_tau=8.0)),
+             ("tcgen05 CNN + tensor-memory 3xTF32 Pfaffian (pf_mode 1)",
+              dict(cnn_mode=2, pf_mode=1))]
+    out = {}
+    ref = None
+    for name, kw in forms:
+        model = nh.PfaffianBackflow(L, L, NE, NE, params=params, device=dev, **kw)
+        state = nh.Variational(model, symm=True, max_parallel=BATCH)
+        ms, _ = time_amplitudes(state, spins, 3, 1, flush, st)
+        psi = state(spins)
+        sg, la = psi.sign.cpu().numpy(), psi.logabs.cpu().numpy()
+        fl = psi.flags.cpu().numpy()
+        if ref is None:
+            ref = (sg, la)
+        out[name] = {"amplitudes_per_s": BATCH * IMAGES / (ms / 3 / 1e3),
+                     "refined_configurations": float(((fl & 8) != 0).mean()),
+                     **_err_stats(la, ref[1], sg, ref[0])}
+        del model, state, psi
+    # near-nodal pairing matrices at the slogpf boundary
+    g = torch.Generator(device=dev)
+    g.manual_seed(3)
+    B, n = 8192, N_OCC
+    A = torch.randn((B, n, n), generator=g, device=dev)
+    A = A - A.transpose(1, 2)
+    nn_idx = torch.arange(0, B, 100, device=dev)  # 1% near-nodal
+    Q, _ = torch.linalg.qr(torch.randn((len(nn_idx), n, n), generator=g, device=dev,
+                                       dtype=torch.float64))
+    a = (torch.rand((len(nn_idx), n // 2), generator=g, device=dev, dtype=torch.float64) * 1.5
+         + 0.5) * torch.where(torch.rand((len(nn_idx), n // 2), generator=g, device=dev) < 0.5,
+                              -1.0, 1.0).double()
+    a[:, 7] *= 1e-6
+    Bm = torch.zeros((len(nn_idx), n, n), dtype=torch.float64, device=dev)
+    k = torch.arange(n // 2, device=dev)
+    Bm[:, 2 * k, 2 * k + 1] = a
+    Bm[:, 2 * k + 1, 2 * k] = -a
+    An = Q.transpose(1, 2) @ Bm @ Q
+    A[nn_idx] = (0.5 * (An - An.transpose(1, 2))).float()
+    s0, l0, _ = nh.slogpf(A, cond_tau=1.0)
+    s1, l1, f1 = nh.slogpf(A)
+    s2, l2, _ = nh.slogpf(A, cond_tau=0.0)
+    refined = (f1.cpu().numpy() & 8) != 0
+    near = np.zeros(B, bool)
+    near[nn_idx.cpu().numpy()] = True
+    out["near-nodal slogpf, 8192 x 224x224 (1% seeded, pivot 1e-6)"] = {
+        "default (FP64 recompute of pivot ratio > 100)":
+            _err_stats(l1.cpu().numpy(), l0.cpu().numpy(), s1.cpu().numpy(), s0.cpu().numpy()),
+        "FP32 only": _err_stats(l2.cpu().numpy(), l0.cpu().numpy(), s2.cpu().numpy(),
+                                s0.cpu().numpy()),
+        "near-nodal refined": int(refined[near].sum()), "near-nodal": int(near.sum()),
+        "refined fraction": float(refined.mean())}
+    del A
+    torch.cuda.empty_cache()
+    out["reference"] = ("all-FP64 path of the library (FP64 CNN, gather and Pfaffian), which "
+                        "matches the numpy oracle to 1e-9 in the parity tests")
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -473,6 +556,9 @@ def run_ours(args) -> None:
     local_energy = None
     if world == 1 and not args.no_eloc:
         local_energy = measure_local_energy(args, dev, st)
+    precision = None
+    if world == 1 and not args.no_precision:
+        precision = measure_precision(dev, st, spins, flush)
 
     if rank == 0:
         cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
@@ -497,6 +583,7 @@ def run_ours(args) -> None:
                     "d2h_bytes_per_step": BATCH * (4 + 8)},
             "sampling": sampling,
             "local_energy": local_energy,
+            "precision": precision,
             "roofline": roof, "kernels": kernels, "gpu_launches": launches,
             "cpu_baseline": cpu, "clocks": clk,
         }
@@ -550,6 +637,8 @@ def main():
     ap.add_argument("--no-eloc", action="store_true",
                     help="skip the ragged local-energy measurement (8x8 and 16x16)")
     ap.add_argument("--eloc-samples", type=int, default=4096)
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the precision-form report (errors against the all-FP64 path)")
     ap.add_argument("--chains", type=int, default=1024)
     ap.add_argument("--sampler-steps", type=int, default=2000)
     ap.add_argument("--burn", type=int, default=6000)

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define NH_ABI_VERSION 2
+#define NH_ABI_VERSION 3
 
 enum {
   NH_OK = 0,
@@ -45,7 +45,8 @@ enum {
   NH_FLAG_ZERO_PIVOT = 1,  /* exactly singular pairing block: sign 0, logabs -inf */
   NH_FLAG_NONFINITE = 2,   /* a non-finite value met during the factorisation */
   NH_FLAG_GROWTH = 4,      /* pivot ratio above cond_tau (near-nodal, ill-conditioned block) */
-  NH_FLAG_REFINED = 8      /* recomputed in FP64 because of NH_FLAG_GROWTH */
+  NH_FLAG_REFINED = 8,     /* recomputed in FP64 because of NH_FLAG_GROWTH */
+  NH_FLAG_CANCEL = 16      /* projected amplitude: sum_g |psi_g| > cancel_tau |sum_g eta_g psi_g| */
 };
 
 /* Parameters of the backflow network (device pointers).
@@ -66,7 +67,12 @@ enum {
  * cond_tau:      an item whose largest / smallest pivot magnitude exceeds cond_tau is flagged
  *                NH_FLAG_GROWTH and, when Wt64 is set and the FP64 kernels fit in shared
  *                memory (n <= 232, N <= 256 at 32 channels), recomputed end to end in FP64
- *                (CNN, gather, Pfaffian; NH_FLAG_REFINED); <= 0 disables both. */
+ *                (CNN, gather, Pfaffian; NH_FLAG_REFINED); <= 0 disables both.
+ * cancel_tau:    projected amplitudes only: a configuration whose 8 images cancel, i.e.
+ *                sum_g |psi(g s)| > cancel_tau |sum_g eta_g psi(g s)|, amplifies the FP32
+ *                error of its images by that factor; with cancel_tau > 0 (and Wt64 set) all its
+ *                images are recomputed in FP64 and the output carries NH_FLAG_CANCEL.  <= 0:
+ *                off (the flag is then never set). */
 typedef struct {
   const float* conv_w;
   const float* conv_b;
@@ -81,6 +87,7 @@ typedef struct {
   int32_t cnn_mode;
   int32_t pf_mode;
   double cond_tau;
+  double cancel_tau;
 } nh_backflow_params;
 
 /* Hubbard model H = -sum t_ij c+_i c_j + U sum n_up n_dn; n_dirs = 4 (nearest) or 8

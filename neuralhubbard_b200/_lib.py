@@ -14,7 +14,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libnh_b200.so")
 
 NH_OK = 0
-FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH, FLAG_REFINED = 1, 2, 4, 8
+FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH, FLAG_REFINED, FLAG_CANCEL = 1, 2, 4, 8, 16
 
 c_void_p, c_int, c_int64, c_uint64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64
 c_float, c_double, c_size_t = ctypes.c_float, ctypes.c_double, ctypes.c_size_t
@@ -41,6 +41,7 @@ class BackflowParams(ctypes.Structure):
         ("cnn_mode", ctypes.c_int32),
         ("pf_mode", ctypes.c_int32),
         ("cond_tau", c_double),
+        ("cancel_tau", c_double),
     ]
 
 

@@ -149,15 +149,18 @@ class PfaffianBackflow:
     def __init__(self, Lx: int, Ly: int, n_up: int, n_dn: int, params: Optional[dict] = None,
                  channels: int = 32, layers: int = 4, seed: int = 0, device="cuda",
                  cond_tau: float = DEFAULT_COND_TAU, cnn_mode: int = 0,
-                 pf_mode: int = 0):
+                 pf_mode: int = 0, cancel_tau: float = 0.0):
         """``cond_tau``: items whose pivot ratio exceeds it are recomputed end to end in FP64
         (``0`` keeps every item on the FP32 path).  ``cnn_mode``: 0 FP32 CUDA cores, 1 tcgen05
         BF16, 2 tcgen05 BF16 x3 (near-FP32); modes 1 and 2 need 16x16, 32 channels, 4 layers.
-        ``pf_mode``: 0 Pfaffian on CUDA cores, 1 matrix in tensor memory with tcgen05 updates."""
+        ``pf_mode``: 0 Pfaffian on CUDA cores, 1 matrix in tensor memory with tcgen05 updates.
+        ``cancel_tau`` (projected amplitudes): configurations whose images cancel by more than
+        this factor are recomputed in FP64 (0 = off)."""
         self.device = torch.device(device)
         self.cond_tau = float(cond_tau)
         self.cnn_mode = int(cnn_mode)
         self.pf_mode = int(pf_mode)
+        self.cancel_tau = float(cancel_tau)
         if params is None:
             params = init_params(Lx, Ly, channels, layers, seed=seed)
         self.channels = int(params["conv_w"][0].shape[0])
@@ -192,7 +195,7 @@ class PfaffianBackflow:
                                    self.conv_w_packed.data_ptr(), _ptr(self.conv_w_tc),
                                    self.Wt.data_ptr(), self.Wt64.data_ptr(), g.LX, g.LY, g.n_up,
                                    g.n_dn, self.channels, self.layers, self.cnn_mode, self.pf_mode,
-                                   self.cond_tau)
+                                   self.cond_tau, self.cancel_tau)
 
     def features(self, spins: torch.Tensor) -> torch.Tensor:
         """(B, 2, N, d) backflow features of int8 configurations (B, 2N)."""

@@ -140,7 +140,11 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
   if ((rc = p.pf_mode == 1 ? launch_pfaffian_tc(g, 1, nullptr, b.err, st)
                            : launch_pfaffian_gather(g, st)))
     return rc;
-  if (p.Wt64 && p.cond_tau > 0.0 && pfaffian64_fits(n) && cnn64_fits(p.Lx * p.Ly, p.channels)) {
+  if (p.Wt64 && (p.cond_tau > 0.0 || (p.cancel_tau > 0.0 && cl.G > 1)) && pfaffian64_fits(n) &&
+      cnn64_fits(p.Lx * p.Ly, p.channels)) {
+    if ((rc = launch_cancel_mark(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev,
+                                 p.cancel_tau, st)))
+      return rc;
     if ((rc = launch_flagged(b.pf_flags, max_items, cl.n_cfg_dev, cl.G, b.list, b.count, st)))
       return rc;
     CnnLaunch c64{&cl, &p, 1, true, b.list, b.count, max_items, nullptr, b.Y64, b.idx64,
@@ -152,7 +156,7 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
     if ((rc = launch_pfaffian_gather(g64, st))) return rc;
   }
   return launch_combine(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev, sign,
-                        logabs, flags, st);
+                        logabs, flags, p.cancel_tau, st);
 }
 
 static int check_params(const nh_backflow_params* p) {

@@ -496,26 +496,56 @@ __global__ void __launch_bounds__(kNumThreads) pairing_kernel(const float* __res
 
 // ------------------------------------------------------------------ image combination
 // Also used with G = 1 to copy the per-item results into the caller's arrays.
+// Sum over the images of one configuration in FP64: returns sum_g s_g exp(l_g - m) and sets
+// *asum to sum_g |.| and *m to the largest log.
+__device__ __forceinline__ double image_sum(const float* __restrict__ sg,
+                                           const double* __restrict__ la, int c, int G,
+                                           double* m_out, double* asum) {
+  double m = -INFINITY;
+  for (int g = 0; g < G; ++g) {
+    const float s = sg[(size_t)c * G + g];
+    const double l = la[(size_t)c * G + g];
+    if (s != 0.0f && l > m) m = l;
+  }
+  double tot = 0.0, a = 0.0;
+  if (m > -INFINITY)
+    for (int g = 0; g < G; ++g) {
+      const float s = sg[(size_t)c * G + g];
+      if (s != 0.0f) {
+        const double t = exp(la[(size_t)c * G + g] - m);
+        tot += (double)s * t;
+        a += t;
+      }
+    }
+  *m_out = m;
+  *asum = a;
+  return tot;
+}
+
+__global__ void cancel_mark_kernel(const float* __restrict__ sg, const double* __restrict__ la,
+                                   int32_t* __restrict__ fl, int G, int n_cfg,
+                                   const int32_t* n_cfg_dev, double cancel_tau) {
+  const int n = n_cfg_dev ? *n_cfg_dev : n_cfg;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    double m, a;
+    const double tot = image_sum(sg, la, c, G, &m, &a);
+    if (a > 0.0 && a > cancel_tau * fabs(tot))
+      for (int g = 0; g < G; ++g) fl[(size_t)c * G + g] |= NH_FLAG_GROWTH | NH_FLAG_CANCEL;
+  }
+}
+
 __global__ void combine_kernel(const float* __restrict__ sg, const double* __restrict__ la,
                                const int32_t* __restrict__ fl, int G, int n_cfg,
                                const int32_t* n_cfg_dev, float* sign, double* logabs,
-                               int32_t* flags) {
+                               int32_t* flags, double cancel_tau) {
   const int n = n_cfg_dev ? *n_cfg_dev : n_cfg;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-    double m = -INFINITY;
     int f = 0;
-    for (int g = 0; g < G; ++g) {
-      const float s = sg[(size_t)c * G + g];
-      const double l = la[(size_t)c * G + g];
-      if (s != 0.0f && l > m) m = l;
-      if (fl) f |= fl[(size_t)c * G + g];
-    }
-    double tot = 0.0;
-    if (m > -INFINITY)
-      for (int g = 0; g < G; ++g) {
-        const float s = sg[(size_t)c * G + g];
-        if (s != 0.0f) tot += (double)s * exp(la[(size_t)c * G + g] - m);
-      }
+    if (fl)
+      for (int g = 0; g < G; ++g) f |= fl[(size_t)c * G + g];
+    double m, a;
+    const double tot = image_sum(sg, la, c, G, &m, &a);
+    if (cancel_tau > 0.0 && a > 0.0 && a > cancel_tau * fabs(tot)) f |= NH_FLAG_CANCEL;
     const float so = tot > 0.0 ? 1.0f : (tot < 0.0 ? -1.0f : 0.0f);
     sign[c] = so;
     logabs[c] = so != 0.0f ? log(fabs(tot)) + m - log((double)G) : -INFINITY;
@@ -1037,12 +1067,22 @@ int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, 
 
 int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, int n_cfg,
                    const int32_t* n_cfg_dev, float* sign, double* logabs, int32_t* flags,
-                   cudaStream_t st) {
+                   double cancel_tau, cudaStream_t st) {
   if (n_cfg <= 0) return NH_OK;
   int grid = (n_cfg + 255) / 256;
   ProfScope prof_scope(NH_K_COMBINE, st);
-  combine_kernel<<<grid, 256, 0, st>>>(sg, la, fl, G, n_cfg, n_cfg_dev, sign, logabs, flags);
+  combine_kernel<<<grid, 256, 0, st>>>(sg, la, fl, G, n_cfg, n_cfg_dev, sign, logabs, flags,
+                                       G > 1 ? cancel_tau : 0.0);
   return check_launch("combine_kernel");
+}
+
+int launch_cancel_mark(const float* sg, const double* la, int32_t* fl, int G, int n_cfg,
+                       const int32_t* n_cfg_dev, double cancel_tau, cudaStream_t st) {
+  if (n_cfg <= 0 || G <= 1 || cancel_tau <= 0.0) return NH_OK;
+  int grid = (n_cfg + 255) / 256;
+  ProfScope prof_scope(NH_K_COMBINE, st);
+  cancel_mark_kernel<<<grid, 256, 0, st>>>(sg, la, fl, G, n_cfg, n_cfg_dev, cancel_tau);
+  return check_launch("cancel_mark_kernel");
 }
 
 int launch_flagged(const int32_t* flags, int n_items, const int32_t* count_dev, int count_mult,

@@ -419,3 +419,27 @@ def test_local_energy_chunk_autotune():
     assert best in (1024, 4096, 16384)
     e = H.Oloc(state, smp)  # uses the tuned chunk
     assert torch.allclose(e, ref, rtol=1e-12, atol=0)
+
+
+def test_cancellation_recompute():
+    """cancel_tau: configurations whose 8 images cancel are recomputed in FP64 image by image;
+    their projected amplitude then equals the all-FP64 result bit for bit, and no configuration
+    is worse than without the recompute."""
+    L, ne = 16, 112
+    params = nh.init_params(L, L, channels=32, std=0.02, seed=0)
+    s = torch.from_numpy(nh.random_spins(np.random.default_rng(1000), 512, L * L, ne, ne)).to(DEV)
+    ref = nh.Variational(nh.PfaffianBackflow(L, L, ne, ne, params=params, cond_tau=1.0),
+                         symm=True)(s)
+    base = nh.Variational(nh.PfaffianBackflow(L, L, ne, ne, params=params), symm=True)(s)
+    m = nh.PfaffianBackflow(L, L, ne, ne, params=params, cancel_tau=8.0)
+    psi = nh.Variational(m, symm=True)(s)
+    fl = psi.flags.cpu().numpy()
+    cancel = (fl & _lib.FLAG_CANCEL) != 0
+    assert 0 < cancel.sum() < len(fl)
+    assert np.all(fl[cancel] & _lib.FLAG_REFINED)
+    la, l0, lb = psi.logabs.cpu().numpy(), ref.logabs.cpu().numpy(), base.logabs.cpu().numpy()
+    assert np.array_equal(la[cancel], l0[cancel])
+    assert torch.equal(psi.sign, ref.sign)
+    assert np.all(np.abs(la - l0) <= np.abs(lb - l0) + 1e-12)
+    # the flag reports the cancellation factor of the final amplitude
+    assert not (base.flags.cpu().numpy() & _lib.FLAG_CANCEL).any()
