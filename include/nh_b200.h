@@ -67,7 +67,10 @@ enum {
  * cond_tau:      an item whose largest / smallest pivot magnitude exceeds cond_tau is flagged
  *                NH_FLAG_GROWTH and, when Wt64 is set and the FP64 kernels fit in shared
  *                memory (n <= 232, N <= 256 at 32 channels), recomputed end to end in FP64
- *                (CNN, gather, Pfaffian; NH_FLAG_REFINED); <= 0 disables both.
+ *                (CNN, gather, Pfaffian; NH_FLAG_REFINED); <= 0 disables both.  For projected
+ *                amplitudes with cond_tau > 1 an image whose |psi(g s)| is below 1e-3 of
+ *                |psi_P(s)| is not recomputed (its error cannot move log|psi_P| by more than
+ *                ~1e-5); cond_tau <= 1 recomputes every image (the all-FP64 form).
  * cancel_tau:    projected amplitudes only: a configuration whose 8 images cancel, i.e.
  *                sum_g |psi(g s)| > cancel_tau |sum_g eta_g psi(g s)|, amplifies the FP32
  *                error of its images by that factor; with cancel_tau > 0 (and Wt64 set) all its

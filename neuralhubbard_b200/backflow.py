@@ -118,6 +118,9 @@ def pairing_occ(Y: torch.Tensor, idx: torch.Tensor, Wt: torch.Tensor, geom: Pair
 
 
 DEFAULT_COND_TAU = 100.0
+# Projected amplitudes whose 8 images cancel by more than this factor are recomputed in FP64:
+# the cancellation amplifies the FP32 error of the images by the same factor.
+DEFAULT_CANCEL_TAU = 8.0
 
 
 def slogpf(F: torch.Tensor, cond_tau: float = DEFAULT_COND_TAU):
@@ -149,13 +152,13 @@ class PfaffianBackflow:
     def __init__(self, Lx: int, Ly: int, n_up: int, n_dn: int, params: Optional[dict] = None,
                  channels: int = 32, layers: int = 4, seed: int = 0, device="cuda",
                  cond_tau: float = DEFAULT_COND_TAU, cnn_mode: int = 0,
-                 pf_mode: int = 0, cancel_tau: float = 0.0):
+                 pf_mode: int = 0, cancel_tau: float = DEFAULT_CANCEL_TAU):
         """``cond_tau``: items whose pivot ratio exceeds it are recomputed end to end in FP64
         (``0`` keeps every item on the FP32 path).  ``cnn_mode``: 0 FP32 CUDA cores, 1 tcgen05
         BF16, 2 tcgen05 BF16 x3 (near-FP32); modes 1 and 2 need 16x16, 32 channels, 4 layers.
         ``pf_mode``: 0 Pfaffian on CUDA cores, 1 matrix in tensor memory with tcgen05 updates.
         ``cancel_tau`` (projected amplitudes): configurations whose images cancel by more than
-        this factor are recomputed in FP64 (0 = off)."""
+        this factor are recomputed in FP64 (0 = off; default 8)."""
         self.device = torch.device(device)
         self.cond_tau = float(cond_tau)
         self.cnn_mode = int(cnn_mode)

@@ -142,8 +142,9 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
     return rc;
   if (p.Wt64 && (p.cond_tau > 0.0 || (p.cancel_tau > 0.0 && cl.G > 1)) && pfaffian64_fits(n) &&
       cnn64_fits(p.Lx * p.Ly, p.channels)) {
-    if ((rc = launch_cancel_mark(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev,
-                                 p.cancel_tau, st)))
+    // cond_tau <= 1 flags every image (the all-FP64 form): nothing is pruned then.
+    if ((rc = launch_image_mark(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev,
+                                p.cancel_tau, p.cond_tau > 1.0, st)))
       return rc;
     if ((rc = launch_flagged(b.pf_flags, max_items, cl.n_cfg_dev, cl.G, b.list, b.count, st)))
       return rc;

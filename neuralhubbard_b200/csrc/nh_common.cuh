@@ -192,10 +192,11 @@ int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, 
 int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, int n_cfg,
                    const int32_t* n_cfg_dev, float* sign, double* logabs, int32_t* flags,
                    double cancel_tau, cudaStream_t st);
-// Marks every image of a configuration whose images cancel (sum |.| > cancel_tau |sum|) with
-// NH_FLAG_GROWTH | NH_FLAG_CANCEL, so that the FP64 recompute list takes them.
-int launch_cancel_mark(const float* sg, const double* la, int32_t* fl, int G, int n_cfg,
-                       const int32_t* n_cfg_dev, double cancel_tau, cudaStream_t st);
+// Projected amplitudes (G > 1): marks every image of a configuration whose images cancel
+// (sum |.| > cancel_tau |sum|) with NH_FLAG_GROWTH | NH_FLAG_CANCEL, and unmarks ill-conditioned
+// images too small to matter, before the FP64 recompute list is built.
+int launch_image_mark(const float* sg, const double* la, int32_t* fl, int G, int n_cfg,
+                      const int32_t* n_cfg_dev, double cancel_tau, bool prune, cudaStream_t st);
 int launch_flagged(const int32_t* flags, int n_items, const int32_t* count_dev, int count_mult,
                    int32_t* list, int32_t* count, cudaStream_t st);
 int launch_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, double* Wt64,

@@ -522,15 +522,30 @@ __device__ __forceinline__ double image_sum(const float* __restrict__ sg,
   return tot;
 }
 
-__global__ void cancel_mark_kernel(const float* __restrict__ sg, const double* __restrict__ la,
-                                   int32_t* __restrict__ fl, int G, int n_cfg,
-                                   const int32_t* n_cfg_dev, double cancel_tau) {
+// Recompute selection for projected amplitudes, before the FP64 list is built: every image of a
+// configuration whose images cancel (sum |.| > cancel_tau |sum|, cancel_tau > 0) is marked; an
+// ill-conditioned image (NH_FLAG_GROWTH) whose share |psi_g| / |sum_g eta_g psi_g| is below
+// kImageWeightFloor is unmarked, since even a 1e-2 error in it moves log|psi_P| by < 1e-5.
+constexpr double kImageWeightFloor = 1e-3;
+
+__global__ void image_mark_kernel(const float* __restrict__ sg, const double* __restrict__ la,
+                                  int32_t* __restrict__ fl, int G, int n_cfg,
+                                  const int32_t* n_cfg_dev, double cancel_tau, bool prune) {
   const int n = n_cfg_dev ? *n_cfg_dev : n_cfg;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     double m, a;
     const double tot = image_sum(sg, la, c, G, &m, &a);
-    if (a > 0.0 && a > cancel_tau * fabs(tot))
+    if (cancel_tau > 0.0 && a > 0.0 && a > cancel_tau * fabs(tot)) {
       for (int g = 0; g < G; ++g) fl[(size_t)c * G + g] |= NH_FLAG_GROWTH | NH_FLAG_CANCEL;
+    } else if (prune && tot != 0.0) {
+      for (int g = 0; g < G; ++g) {
+        const size_t i = (size_t)c * G + g;
+        const int f = fl[i];
+        if ((f & NH_FLAG_GROWTH) && !(f & NH_FLAG_NONFINITE) && sg[i] != 0.0f &&
+            exp(la[i] - m) < kImageWeightFloor * fabs(tot))
+          fl[i] = f & ~NH_FLAG_GROWTH;
+      }
+    }
   }
 }
 
@@ -1076,13 +1091,13 @@ int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, 
   return check_launch("combine_kernel");
 }
 
-int launch_cancel_mark(const float* sg, const double* la, int32_t* fl, int G, int n_cfg,
-                       const int32_t* n_cfg_dev, double cancel_tau, cudaStream_t st) {
-  if (n_cfg <= 0 || G <= 1 || cancel_tau <= 0.0) return NH_OK;
+int launch_image_mark(const float* sg, const double* la, int32_t* fl, int G, int n_cfg,
+                      const int32_t* n_cfg_dev, double cancel_tau, bool prune, cudaStream_t st) {
+  if (n_cfg <= 0 || G <= 1 || (cancel_tau <= 0.0 && !prune)) return NH_OK;
   int grid = (n_cfg + 255) / 256;
   ProfScope prof_scope(NH_K_COMBINE, st);
-  cancel_mark_kernel<<<grid, 256, 0, st>>>(sg, la, fl, G, n_cfg, n_cfg_dev, cancel_tau);
-  return check_launch("cancel_mark_kernel");
+  image_mark_kernel<<<grid, 256, 0, st>>>(sg, la, fl, G, n_cfg, n_cfg_dev, cancel_tau, prune);
+  return check_launch("image_mark_kernel");
 }
 
 int launch_flagged(const int32_t* flags, int n_items, const int32_t* count_dev, int count_mult,
