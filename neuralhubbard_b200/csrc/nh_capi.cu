@@ -85,16 +85,17 @@ int num_sms() {
 
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-size_t pipeline_bytes(int max_items, int n, int d) {
+size_t pipeline_bytes(int max_items, int n, int d, int N, int C) {
   const size_t it = (size_t)(max_items > 0 ? max_items : 1);
   return align256(it * n * d * sizeof(float)) + align256(it * n * sizeof(int32_t)) +
          align256(it * sizeof(float)) * 2 + align256(it * sizeof(double)) +
          align256(it * sizeof(int32_t)) * 2 + align256(sizeof(int32_t)) +
          align256(it * n * d * sizeof(double)) + align256(it * n * sizeof(int32_t)) +
-         align256(sizeof(int32_t));
+         align256(sizeof(int32_t)) + align256(pfaffian_scratch_bytes(n)) +
+         align256(cnn_scratch_bytes(N, C));
 }
 
-PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d) {
+PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d, int N, int C) {
   const size_t it = (size_t)(max_items > 0 ? max_items : 1);
   char* p = static_cast<char*>(ws);
   auto take = [&](size_t bytes) {
@@ -114,6 +115,9 @@ PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d) {
   b.Y64 = reinterpret_cast<double*>(take(it * n * d * sizeof(double)));
   b.idx64 = reinterpret_cast<int32_t*>(take(it * n * sizeof(int32_t)));
   b.err = reinterpret_cast<int32_t*>(take(sizeof(int32_t)));
+  const size_t tri_bytes = pfaffian_scratch_bytes(n), act_bytes = cnn_scratch_bytes(N, C);
+  b.pf_tri = tri_bytes ? take(tri_bytes) : nullptr;
+  b.cnn_act = act_bytes ? take(act_bytes) : nullptr;
   return b;
 }
 
@@ -131,17 +135,17 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
   if (p.cnn_mode == 1 || p.cnn_mode == 2) {
     rc = launch_cnn_tc(cl, p, p.cnn_mode, b.Y, b.idx, b.item_sign, b.err, st);
   } else {
-    CnnLaunch c{&cl, &p, 1, false, nullptr, nullptr, 0, nullptr, b.Y, b.idx, b.item_sign};
+    CnnLaunch c{&cl, &p, 1, false, nullptr, nullptr, 0, nullptr, b.Y, b.idx, b.item_sign,
+                b.cnn_act};
     rc = launch_cnn(c, st);
   }
   if (rc) return rc;
   PfGatherArgs g{b.Y, b.idx, p.Wt, p.Lx, p.Ly, d, n, cl.n_cfg_dev, cl.G, max_items, nullptr,
-                 b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, p.cond_tau, 0, false};
+                 b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, p.cond_tau, 0, false, b.pf_tri};
   if ((rc = p.pf_mode == 1 ? launch_pfaffian_tc(g, 1, nullptr, b.err, st)
                            : launch_pfaffian_gather(g, st)))
     return rc;
-  if (p.Wt64 && (p.cond_tau > 0.0 || (p.cancel_tau > 0.0 && cl.G > 1)) && pfaffian64_fits(n) &&
-      cnn64_fits(p.Lx * p.Ly, p.channels)) {
+  if (p.Wt64 && (p.cond_tau > 0.0 || (p.cancel_tau > 0.0 && cl.G > 1))) {
     // cond_tau <= 1 flags every image (the all-FP64 form): nothing is pruned then.
     if ((rc = launch_image_mark(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev,
                                 p.cancel_tau, p.cond_tau > 1.0, st)))
@@ -149,11 +153,11 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
     if ((rc = launch_flagged(b.pf_flags, max_items, cl.n_cfg_dev, cl.G, b.list, b.count, st)))
       return rc;
     CnnLaunch c64{&cl, &p, 1, true, b.list, b.count, max_items, nullptr, b.Y64, b.idx64,
-                  b.item_sign};
+                  b.item_sign, b.cnn_act};
     if ((rc = launch_cnn(c64, st))) return rc;
     PfGatherArgs g64{b.Y64, b.idx64, p.Wt64, p.Lx, p.Ly, d, n, b.count, 1, max_items, b.list,
                      b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, 0.0,
-                     NH_FLAG_GROWTH | NH_FLAG_REFINED, true};
+                     NH_FLAG_GROWTH | NH_FLAG_REFINED, true, b.pf_tri};
     if ((rc = launch_pfaffian_gather(g64, st))) return rc;
   }
   return launch_combine(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev, sign,
@@ -166,9 +170,9 @@ static int check_params(const nh_backflow_params* p) {
   if (p->Lx < 3 || p->Ly < 3 || p->Lx > 32 || p->Ly > 32)
     return fail(NH_ERR_UNSUPPORTED, "lattice %dx%d (3 <= Lx, Ly <= 32)", p->Lx, p->Ly);
   const int n = p->n_up + p->n_dn;
-  if (p->n_up < 0 || p->n_dn < 0 || n < 2 || n % 2 || n > kNumThreads)
+  if (p->n_up < 0 || p->n_dn < 0 || n < 2 || n % 2 || n > kMaxN)
     return fail(NH_ERR_UNSUPPORTED, "electrons %d + %d (even total <= %d)", p->n_up, p->n_dn,
-                kNumThreads);
+                kMaxN);
   const int d = p->channels / 2;
   if (p->channels % 2 || (d != 8 && d != 16 && d != 32))
     return fail(NH_ERR_UNSUPPORTED, "channels %d (16, 32 or 64)", p->channels);
@@ -180,6 +184,8 @@ static int check_params(const nh_backflow_params* p) {
   if (p->cnn_mode && !p->conv_w_tc) return fail(NH_ERR_INVALID, "cnn_mode %d: conv_w_tc is null",
                                                 p->cnn_mode);
   if (p->pf_mode < 0 || p->pf_mode > 1) return fail(NH_ERR_INVALID, "pf_mode %d", p->pf_mode);
+  if (p->pf_mode == 1 && n > kNumThreads)
+    return fail(NH_ERR_UNSUPPORTED, "pf_mode 1 needs n <= %d", kNumThreads);
   return NH_OK;
 }
 
@@ -261,7 +267,8 @@ int nh_cnn_forward(const int8_t* spins, int batch, const nh_backflow_params* p, 
   if (p->Lx < 3 || p->Ly < 3 || p->Lx > 32 || p->Ly > 32)
     return fail(NH_ERR_UNSUPPORTED, "cnn_forward: lattice %dx%d", p->Lx, p->Ly);
   ConfigList cl{spins, nullptr, nullptr, nullptr, nullptr, batch, 1};
-  CnnLaunch c{&cl, p, 0, false, nullptr, nullptr, 0, features, nullptr, nullptr, nullptr};
+  CnnLaunch c{&cl, p, 0, false, nullptr, nullptr, 0, features, nullptr, nullptr, nullptr,
+              nullptr};
   return launch_cnn(c, static_cast<cudaStream_t>(stream));
 }
 
@@ -300,7 +307,8 @@ int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, do
 
 size_t nh_amplitude_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p) {
   if (!p) return 0;
-  return pipeline_bytes(batch * n_symm, p->n_up + p->n_dn, p->channels / 2);
+  return pipeline_bytes(batch * n_symm, p->n_up + p->n_dn, p->channels / 2, p->Lx * p->Ly,
+                        p->channels);
 }
 
 int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_params* p,
@@ -315,7 +323,7 @@ int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_p
   if (!workspace || workspace_bytes < need)
     return fail(NH_ERR_WORKSPACE, "amplitude: workspace %zu < %zu bytes", workspace_bytes, need);
   const int n = p->n_up + p->n_dn, d = p->channels / 2;
-  PipelineBuffers b = carve_pipeline(workspace, batch * n_symm, n, d);
+  PipelineBuffers b = carve_pipeline(workspace, batch * n_symm, n, d, p->Lx * p->Ly, p->channels);
   ConfigList cl{spins, nullptr, nullptr, nullptr, nullptr, batch, n_symm};
   return run_pipeline(cl, *p, b, sign, logabs, flags, static_cast<cudaStream_t>(stream));
 }
@@ -361,7 +369,7 @@ static ElocLayout eloc_layout(void* ws, int batch, int n_symm, int chunk,
   L.clogabs = reinterpret_cast<double*>(take(cmax * 8));
   L.n_chunks = (int)((cmax + chunk - 1) / chunk);
   L.chunk_cnt = reinterpret_cast<int32_t*>(take((size_t)L.n_chunks * 4));
-  L.pipe = take(pipeline_bytes(chunk * n_symm, n, d));
+  L.pipe = take(pipeline_bytes(chunk * n_symm, n, d, p->Lx * p->Ly, p->channels));
   L.bytes = off;
   return L;
 }
@@ -416,7 +424,7 @@ int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs
     *n_conn_out = total;
     used = (int)((total + chunk - 1) / chunk);
   }
-  PipelineBuffers b = carve_pipeline(L.pipe, chunk * n_symm, n, d);
+  PipelineBuffers b = carve_pipeline(L.pipe, chunk * n_symm, n, d, N, p->channels);
   for (int i = 0; i < used; ++i) {
     const int64_t c0 = (int64_t)i * chunk;
     ConfigList cl{spins, L.owner + c0, L.from + c0, L.to + c0, L.chunk_cnt + i, chunk, n_symm};
@@ -474,7 +482,7 @@ static MhLayout mh_layout(void* ws, int batch, int n_symm, const nh_backflow_par
   L.psign = reinterpret_cast<float*>(take((size_t)batch * 4));
   L.plogabs = reinterpret_cast<double*>(take((size_t)batch * 8));
   L.lqr = reinterpret_cast<float*>(take((size_t)batch * 4));
-  L.pipe = take(pipeline_bytes(batch * n_symm, n, d));
+  L.pipe = take(pipeline_bytes(batch * n_symm, n, d, p->Lx * p->Ly, p->channels));
   L.bytes = off;
   return L;
 }
@@ -501,7 +509,7 @@ int nh_metropolis_steps(int8_t* spins, float* sign, double* logabs, int batch, i
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   MhLayout L = mh_layout(workspace, batch, n_symm, p);
   const int n = p->n_up + p->n_dn, d = p->channels / 2, N = p->Lx * p->Ly;
-  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, n, d);
+  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, n, d, N, p->channels);
   for (int t = 0; t < nsteps; ++t) {
     const int64_t step = step0 + t;
     if ((rc = launch_mh_propose(spins, batch, p->Lx, p->Ly, n_dirs, seed, step, L.valid, L.from,
@@ -547,7 +555,7 @@ int nh_metropolis_steps_learned(int8_t* spins, float* sign, double* logabs, int 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   MhLayout L = mh_layout(workspace, batch, n_symm, p);
   const int n = p->n_up + p->n_dn, d = p->channels / 2, N = p->Lx * p->Ly;
-  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, n, d);
+  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, n, d, N, p->channels);
   for (int t = 0; t < nsteps; ++t) {
     const int64_t step = step0 + t;
     if ((rc = launch_prop_sample(spins, batch, *q, seed, step, L.valid, L.from, L.to, L.lqr, st)))

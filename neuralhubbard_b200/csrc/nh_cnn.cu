@@ -32,6 +32,7 @@ struct CnnArgs {
   T* Y;
   int32_t* idx;
   float* item_sign;
+  T* act;  // GACT: per-CTA activation planes (2 C (N + 1)) in global memory
 };
 
 __device__ __forceinline__ float gelu_tanh(float x) {
@@ -87,14 +88,23 @@ __device__ __forceinline__ int block_scan(int v, int* warp_buf, int* total) {
   return base + x - v;
 }
 
-template <typename T>
+// GACT: the two activation planes live in a per-CTA slice of global memory (large lattices,
+// where they exceed shared memory); shared memory then holds the weights and scratch only.
+template <typename T, bool GACT = false>
 __global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = a.N, C = a.C, NS = N + 1, M2 = 2 * N;
   const int tid = threadIdx.x;
-  T* actA = reinterpret_cast<T*>(smem_raw);
+  T* actA;
+  T* wsm;  // [ci][tap][co]
+  if constexpr (GACT) {
+    actA = a.act + (size_t)blockIdx.x * 2 * C * NS;
+    wsm = reinterpret_cast<T*>(smem_raw);
+  } else {
+    actA = reinterpret_cast<T*>(smem_raw);
+    wsm = actA + 2 * C * NS;
+  }
   T* actB = actA + C * NS;
-  T* wsm = actB + C * NS;      // [ci][tap][co]
   T* bsm = wsm + C * C * 9;    // [co]
   int* simg = reinterpret_cast<int*>(bsm + C);  // (2N) +-1 of the image configuration
   int* occl = simg + M2;       // (2N) ascending occupied modes of the image configuration
@@ -240,11 +250,13 @@ __global__ void pack_kernel(const float* __restrict__ w, int C, int layers, floa
   }
 }
 
-template <typename T>
+template <typename T, bool GACT = false>
 size_t cnn_smem(int N, int C) {
-  return sizeof(T) * (2 * (size_t)C * (N + 1) + (size_t)C * C * 9 + C) +
+  return sizeof(T) * ((GACT ? 0 : 2 * (size_t)C * (N + 1)) + (size_t)C * C * 9 + C) +
          sizeof(int) * (4 * (size_t)N + 4 * 32 + 32);
 }
+
+constexpr int kCnnBigPerSm = 4;  // CTAs per SM of the global-activation kernel (grid bound)
 
 }  // namespace
 
@@ -257,6 +269,39 @@ int launch_pack_cnn(const float* conv_w, int channels, int layers, float* packed
   return check_launch("pack_kernel");
 }
 
+template <typename T, bool GACT>
+int launch_cnn_t(const CnnLaunch& q, int N, int C, cudaStream_t st) {
+  const nh_backflow_params& p = *q.p;
+  const size_t smem = cnn_smem<T, GACT>(N, C);
+  if (smem > 227 * 1024)
+    return fail(NH_ERR_UNSUPPORTED, "cnn: lattice N=%d with %d channels needs %zu B of smem",
+                N, C, smem);
+  if (GACT && !q.act)
+    return fail(NH_ERR_UNSUPPORTED, "cnn: N=%d needs the large-lattice activation scratch", N);
+  const int slots = q.slot_item ? q.max_slots : q.cl->n_cfg * q.cl->G;
+  if (slots <= 0) return NH_OK;
+  int grid = GACT ? num_sms() * kCnnBigPerSm : num_sms() * (smem > 113 * 1024 ? 1 : 2) * 4;
+  if (grid > slots) grid = slots;
+  static size_t configured = 0;
+  if (smem > 48 * 1024 && smem > configured) {
+    cudaError_t e = cudaFuncSetAttribute(cnn_kernel<T, GACT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return check_cuda(e, "cnn smem attribute");
+    configured = smem;
+  }
+  CnnArgs<T> a{*q.cl, p.conv_w_packed, p.conv_b, p.Lx, p.Ly, N, C, p.layers,
+               p.n_up + p.n_dn, q.mode, q.slot_item, q.slot_count, q.max_slots,
+               q.feat, static_cast<T*>(q.Y), q.idx, q.item_sign, static_cast<T*>(q.act)};
+  ProfScope prof_scope(sizeof(T) == 8 ? NH_K_CNN64 : NH_K_CNN, st);
+  cnn_kernel<T, GACT><<<grid, kNumThreads, smem, st>>>(a);
+  return check_launch(sizeof(T) == 8 ? "cnn_kernel<double>" : "cnn_kernel<float>");
+}
+
+size_t cnn_scratch_bytes(int N, int C) {
+  if (cnn_smem<double>(N, C) <= 227 * 1024) return 0;
+  return (size_t)num_sms() * kCnnBigPerSm * 2 * C * (N + 1) * sizeof(double);
+}
+
 int launch_cnn(const CnnLaunch& q, cudaStream_t st) {
   const nh_backflow_params& p = *q.p;
   const int N = p.Lx * p.Ly, C = p.channels;
@@ -265,43 +310,11 @@ int launch_cnn(const CnnLaunch& q, cudaStream_t st) {
                 C, p.layers, N);
   if (!p.conv_w_packed)
     return fail(NH_ERR_INVALID, "cnn: conv_w_packed is null (call nh_pack_cnn_weights)");
-  const size_t smem = q.fp64 ? cnn_smem<double>(N, C) : cnn_smem<float>(N, C);
-  if (smem > 227 * 1024)
-    return fail(NH_ERR_UNSUPPORTED, "cnn: lattice N=%d with %d channels needs %zu B of smem "
-                "(%s)", N, C, smem, q.fp64 ? "FP64" : "FP32");
-  const int slots = q.slot_item ? q.max_slots : q.cl->n_cfg * q.cl->G;
-  if (slots <= 0) return NH_OK;
-  const int per_sm = smem > 113 * 1024 ? 1 : 2;
-  int grid = num_sms() * per_sm * 4;
-  if (grid > slots) grid = slots;
-  if (q.fp64) {
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
-      cudaError_t e = cudaFuncSetAttribute(cnn_kernel<double>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return check_cuda(e, "cnn smem attribute");
-      configured = smem;
-    }
-    CnnArgs<double> a{*q.cl, p.conv_w_packed, p.conv_b, p.Lx, p.Ly, N, C, p.layers,
-                      p.n_up + p.n_dn, q.mode, q.slot_item, q.slot_count, q.max_slots,
-                      q.feat, static_cast<double*>(q.Y), q.idx, q.item_sign};
-    ProfScope prof_scope(NH_K_CNN64, st);
-    cnn_kernel<double><<<grid, kNumThreads, smem, st>>>(a);
-    return check_launch("cnn_kernel<double>");
-  }
-  static size_t configured = 0;
-  if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(cnn_kernel<float>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "cnn smem attribute");
-    configured = smem;
-  }
-  CnnArgs<float> a{*q.cl, p.conv_w_packed, p.conv_b, p.Lx, p.Ly, N, C, p.layers,
-                   p.n_up + p.n_dn, q.mode, q.slot_item, q.slot_count, q.max_slots,
-                   q.feat, static_cast<float*>(q.Y), q.idx, q.item_sign};
-  ProfScope prof_scope(NH_K_CNN, st);
-  cnn_kernel<float><<<grid, kNumThreads, smem, st>>>(a);
-  return check_launch("cnn_kernel<float>");
+  if (q.fp64)
+    return cnn_smem<double>(N, C) <= 227 * 1024 ? launch_cnn_t<double, false>(q, N, C, st)
+                                                 : launch_cnn_t<double, true>(q, N, C, st);
+  return cnn_smem<float>(N, C) <= 227 * 1024 ? launch_cnn_t<float, false>(q, N, C, st)
+                                              : launch_cnn_t<float, true>(q, N, C, st);
 }
 
 }  // namespace nh

@@ -138,10 +138,12 @@ struct PipelineBuffers {
   double* Y64;        // (items, n, d)
   int32_t* idx64;     // (items, n)
   int32_t* err;       // (1,) device error word of the tensor-core CNN
+  void* pf_tri;       // large lattices: per-CTA Pfaffian triangles (pfaffian_scratch_bytes)
+  void* cnn_act;      // large lattices: per-CTA CNN activation planes (cnn_scratch_bytes)
 };
 
-size_t pipeline_bytes(int max_items, int n, int d);
-PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d);
+size_t pipeline_bytes(int max_items, int n, int d, int N, int C);
+PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d, int N, int C);
 
 // CNN launch: all items of a configuration list (slot = item), or the items of a device list.
 struct CnnLaunch {
@@ -156,6 +158,7 @@ struct CnnLaunch {
   void* Y;                    // float or double (fp64)
   int32_t* idx;
   float* item_sign;
+  void* act;                  // per-CTA activation planes when they exceed shared memory, or null
 };
 
 struct PfGatherArgs {
@@ -174,6 +177,7 @@ struct PfGatherArgs {
   double cond_tau;
   int flag_or;
   bool fp64;
+  void* tri;  // per-CTA triangles for n beyond shared memory (pfaffian_scratch_bytes), or null
 };
 
 // Launchers (return NH_OK or an error code).
@@ -210,6 +214,11 @@ int launch_cnn_tc(const ConfigList& cl, const nh_backflow_params& p, int mode, f
 // Whether the FP64 kernels fit in shared memory (n x n Pfaffian; N sites x C channels CNN).
 bool pfaffian64_fits(int n);
 bool cnn64_fits(int N, int C);
+// Large lattices: bytes of global scratch the Pfaffian (FP32 and FP64) and the CNN need when
+// their working set exceeds shared memory (0 when it does not).
+bool pfaffian_needs_scratch(int n, bool fp64);
+size_t pfaffian_scratch_bytes(int n);
+size_t cnn_scratch_bytes(int N, int C);
 
 // Full amplitude of a configuration list: CNN -> gather + Pfaffian -> image combination.
 int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const PipelineBuffers& b,

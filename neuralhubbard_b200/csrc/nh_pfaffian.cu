@@ -86,6 +86,7 @@ struct PfArgs {
   int32_t* flags;            // (items,) or null
   double cond_tau;           // flag NH_FLAG_GROWTH when max|piv| > cond_tau min|piv| (0: off)
   int flag_or;               // OR-ed into every written flag
+  void* tri;                 // large n: per-CTA lower triangles of T in global memory
 };
 
 __device__ __forceinline__ int tri_off(int i) { return (i * (i - 1)) >> 1; }
@@ -122,12 +123,12 @@ __device__ __forceinline__ T pair_value(const T* yp, int sp, int xp, int ypos,
   return acc;
 }
 
-template <typename T, int D>
+template <typename T, int D, int WARPS = kWarps>
 __device__ void gather_lower(T* Lw, int n, const T* __restrict__ Y, const int32_t* __restrict__ idx,
                              const T* __restrict__ Wt, int Lx, int Ly) {
   const int N = Lx * Ly;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int p = wid; p < n; p += kWarps) {
+  for (int p = wid; p < n; p += WARPS) {
     const int mp = __ldg(idx + p);
     const int sp = mp >= N ? 1 : 0;
     const int sitep = mp - sp * N;
@@ -149,26 +150,39 @@ __device__ void gather_lower(T* Lw, int n, const T* __restrict__ Y, const int32_
   }
 }
 
-template <typename T, int NB, int D>
-__global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
+// THREADS = 256: the lower triangle lives in shared memory (n <= 256).  THREADS = 1024 (large
+// lattices, n <= 1024): one thread per row as well, the triangle in a per-CTA slice of global
+// memory (a.tri; L2-resident up to n ~ 500), shared memory holding only the panel and the
+// reduction slots.
+template <typename T, int NB, int D, int THREADS = kNumThreads>
+__global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T) == 4 ? 2 : 1))
     pfaffian_kernel(PfArgs a) {
   static_assert(NB % Vec<T>::k == 0, "panel width must fill 16-byte vectors");
+  constexpr int WARPS = THREADS / 32;
+  constexpr bool kGlobalTri = THREADS > kNumThreads;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = a.n;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int tri = tri_off(n);
-  T* Lw = reinterpret_cast<T*>(smem_raw);
-  T* Us = Lw + ((tri + 3) & ~3);  // (n, NB)
+  T* Lw;
+  T* Us;  // (n, NB)
+  if constexpr (kGlobalTri) {
+    Lw = static_cast<T*>(a.tri) + (size_t)blockIdx.x * ((tri + 3) & ~3);
+    Us = reinterpret_cast<T*>(smem_raw);
+  } else {
+    Lw = reinterpret_cast<T*>(smem_raw);
+    Us = Lw + ((tri + 3) & ~3);
+  }
   T* Vs = Us + n * NB;            // (n, NB)
   // FP32: the winner's signed value shares the key slot (its magnitude is the key); FP64 keeps
   // it separately.  pivs[k/2] = pivot A[k, k+1], negated when that step swapped labels.
-  constexpr int kValSlots = sizeof(T) == 4 ? 0 : kWarps;
+  constexpr int kValSlots = sizeof(T) == 4 ? 0 : WARPS;
   T* rval = Vs + n * NB;                 // (warps, FP64 only) candidate signed value
   T* pivs = rval + kValSlots;            // (n / 2) signed pivots, multiplied at the end
   float* rkey = reinterpret_cast<float*>(pivs + ((n / 2 + 3) & ~3));  // (warps) candidate key
-  int* rt = reinterpret_cast<int*>(rkey + kWarps);  // (warps) candidate row; later ballot counts
-  int* rlog = rt + kWarps;                          // (warps) candidate logical label
-  int* alist = rlog + kWarps;                       // (n) active physical rows
+  int* rt = reinterpret_cast<int*>(rkey + WARPS);  // (warps) candidate row; later ballot counts
+  int* rlog = rt + WARPS;                          // (warps) candidate logical label
+  int* alist = rlog + WARPS;                       // (n) active physical rows
   int* misc = alist + n;                            // [0] physical row of logical k
 
   const int n_work = a.count_dev ? (*a.count_dev) * a.count_mult : a.n_slots;
@@ -179,14 +193,14 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
     __syncthreads();
     if (a.mode == 0) {
       const float* F = a.F + (size_t)item * n * n;
-      for (int i = wid; i < n; i += kWarps) {
+      for (int i = wid; i < n; i += WARPS) {
         const float* src = F + (size_t)i * n;
         T* dst = Lw + tri_off(i);
         for (int j = lane; j < i; j += 32) dst[j] = T(__ldg(src + j));
       }
     } else {
-      gather_lower<T, D>(Lw, n, Ybase + (size_t)slot * n * D, a.idx + (size_t)slot * n, Wt,
-                         a.Lx, a.Ly);
+      gather_lower<T, D, WARPS>(Lw, n, Ybase + (size_t)slot * n * D, a.idx + (size_t)slot * n,
+                                Wt, a.Lx, a.Ly);
     }
     if (tid == 0) misc[0] = 0;
     __syncthreads();
@@ -233,9 +247,9 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
             }
           }
           __syncthreads();  // (1) pivot candidates
-          float kw[kWarps];
+          float kw[WARPS];
 #pragma unroll
-          for (int w = 0; w < kWarps; w += 4) {
+          for (int w = 0; w < WARPS; w += 4) {
             const float4 q4 = *reinterpret_cast<const float4*>(rkey + w);
             kw[w] = q4.x;
             kw[w + 1] = q4.y;
@@ -245,10 +259,10 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
 
           float bk = kw[0];
 #pragma unroll
-          for (int w = 1; w < kWarps; ++w) bk = fmaxf(bk, kw[w]);
-          int w0 = kWarps - 1;
+          for (int w = 1; w < WARPS; ++w) bk = fmaxf(bk, kw[w]);
+          int w0 = WARPS - 1;
 #pragma unroll
-          for (int w = kWarps - 2; w >= 0; --w) w0 = kw[w] == bk ? w : w0;
+          for (int w = WARPS - 2; w >= 0; --w) w0 = kw[w] == bk ? w : w0;
           const int r = rt[w0];
           const int lw = rlog[w0];
           const int lr = lw & 0x7FFFFFFF;
@@ -298,7 +312,7 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
         __syncthreads();
         int before = 0;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) before += (w < wid) ? rt[w] : 0;
+        for (int w = 0; w < WARPS; ++w) before += (w < wid) ? rt[w] : 0;
         if (on) alist[before + __popc(bal & ((1u << lane) - 1u))] = tid;
         __syncthreads();  // (3) active list in physical order
         // Work units: (64-column block cb, group of RT consecutive rows below its diagonal);
@@ -311,7 +325,7 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
         T ub0[NB], vb0[NB], ub1[NB], vb1[NB];
 #pragma unroll
         for (int p = 0; p < NB; ++p) ub0[p] = vb0[p] = ub1[p] = vb1[p] = T(0);
-        for (int pi = wid; pi < total; pi += kWarps, rem += kWarps) {
+        for (int pi = wid; pi < total; pi += WARPS, rem += WARPS) {
           while (rem >= (m - 64 * cb - 1 + RT - 1) / RT) {
             rem -= (m - 64 * cb - 1 + RT - 1) / RT;
             ++cb;
@@ -410,46 +424,57 @@ __global__ void __launch_bounds__(kNumThreads, sizeof(T) == 4 ? 2 : 1)
   }
 }
 
-template <typename T, int NB>
+template <typename T, int NB, int WARPS = kWarps, bool kGlobalTri = false>
 size_t pf_smem(int n) {
   const size_t tri = (size_t)n * (n - 1) / 2;
-  const size_t val_slots = sizeof(T) == 4 ? 0 : kWarps;
-  return sizeof(T) * (((tri + 3) & ~(size_t)3) + 2 * (size_t)n * NB + val_slots +
-                      ((n / 2 + 3) & ~(size_t)3)) +
-         sizeof(float) * kWarps + sizeof(int) * (2 * kWarps + (size_t)n + 1);
+  const size_t val_slots = sizeof(T) == 4 ? 0 : WARPS;
+  return sizeof(T) * ((kGlobalTri ? 0 : ((tri + 3) & ~(size_t)3)) + 2 * (size_t)n * NB +
+                      val_slots + ((n / 2 + 3) & ~(size_t)3)) +
+         sizeof(float) * WARPS + sizeof(int) * (2 * WARPS + (size_t)n + 1);
 }
 
-template <typename T, int NB, int D>
+// Large lattices: 1024 threads, triangle in a.tri; the panel width that fits shared memory.
+constexpr int kBigThreads = 1024;
+constexpr int kBigNB = 4;
+
+template <typename T, int NB, int D, int THREADS = kNumThreads>
 int launch_pf(const PfArgs& a, cudaStream_t st) {
-  const size_t smem = pf_smem<T, NB>(a.n);
+  constexpr bool kGlobalTri = THREADS > kNumThreads;
+  const size_t smem = pf_smem<T, NB, THREADS / 32, kGlobalTri>(a.n);
   if (smem > 227 * 1024)
     return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d needs %zu B of shared memory", a.n, smem);
+  if (kGlobalTri && !a.tri)
+    return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d needs the large-lattice scratch", a.n);
   static size_t configured = 0;
   if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pfaffian_kernel<T, NB, D>,
+    cudaError_t e = cudaFuncSetAttribute(pfaffian_kernel<T, NB, D, THREADS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return check_cuda(e, "slogpf smem attribute");
     configured = smem;
   }
-  const int per_sm = smem <= 113 * 1024 ? 2 : 1;
+  const int per_sm = (!kGlobalTri && smem <= 113 * 1024) ? 2 : 1;
   int grid = num_sms() * per_sm;
   if (grid > a.n_slots) grid = a.n_slots;
   if (grid <= 0) return NH_OK;
   ProfScope prof_scope(sizeof(T) == 4 ? NH_K_PFAFFIAN : NH_K_PFAFFIAN64, st);
-  pfaffian_kernel<T, NB, D><<<grid, kNumThreads, smem, st>>>(a);
+  pfaffian_kernel<T, NB, D, THREADS><<<grid, THREADS, smem, st>>>(a);
   return check_launch("pfaffian_kernel");
 }
 
-// FP32: the widest panel that keeps two CTAs per SM; FP64: one CTA per SM.
+// FP32: the widest panel that keeps two CTAs per SM; FP64: one CTA per SM; beyond shared
+// memory (FP32 n > 256, FP64 n > 232): the large-lattice kernel.
 template <typename T, int D>
 int launch_pf_pick(const PfArgs& a, cudaStream_t st) {
-  if constexpr (sizeof(T) == 4) {
-    if (pf_smem<T, 8>(a.n) <= 113 * 1024) return launch_pf<T, 8, D>(a, st);
-    return launch_pf<T, 4, D>(a, st);
-  } else {
-    if (pf_smem<T, 4>(a.n) <= 227 * 1024) return launch_pf<T, 4, D>(a, st);
-    return launch_pf<T, 2, D>(a, st);
+  if (a.n <= kNumThreads) {
+    if constexpr (sizeof(T) == 4) {
+      if (pf_smem<T, 8>(a.n) <= 113 * 1024) return launch_pf<T, 8, D>(a, st);
+      return launch_pf<T, 4, D>(a, st);
+    } else {
+      if (pf_smem<T, 4>(a.n) <= 227 * 1024) return launch_pf<T, 4, D>(a, st);
+      if (pf_smem<T, 2>(a.n) <= 227 * 1024) return launch_pf<T, 2, D>(a, st);
+    }
   }
+  return launch_pf<T, kBigNB, D, kBigThreads>(a, st);
 }
 
 template <typename T>
@@ -988,6 +1013,16 @@ int launch_pf_tc(const PfArgs& a, int32_t* err, cudaStream_t st) {
 
 bool pfaffian64_fits(int n) { return pf_smem<double, 2>(n) <= 227 * 1024; }
 
+bool pfaffian_needs_scratch(int n, bool fp64) {
+  if (n > kNumThreads) return true;
+  return fp64 ? pf_smem<double, 2>(n) > 227 * 1024 : pf_smem<float, 4>(n) > 227 * 1024;
+}
+
+size_t pfaffian_scratch_bytes(int n) {
+  const size_t tri = ((size_t)n * (n - 1) / 2 + 3) & ~(size_t)3;
+  return pfaffian_needs_scratch(n, true) ? (size_t)num_sms() * tri * sizeof(double) : 0;
+}
+
 int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list,
                            const int32_t* count, bool fp64, double cond_tau, int flag_or,
                            float* sign, double* logabs, int32_t* flags, cudaStream_t st) {
@@ -1010,8 +1045,8 @@ int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list
 }
 
 int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st) {
-  if (g.n <= 0 || g.n % 2 || g.n > kNumThreads)
-    return fail(NH_ERR_UNSUPPORTED, "amplitude: n=%d must be even and <= %d", g.n, kNumThreads);
+  if (g.n <= 0 || g.n % 2 || g.n > kBigThreads)
+    return fail(NH_ERR_UNSUPPORTED, "amplitude: n=%d must be even and <= %d", g.n, kBigThreads);
   PfArgs a{};
   a.n = g.n;
   a.mode = 1;
@@ -1030,6 +1065,7 @@ int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st) {
   a.flags = g.flags;
   a.cond_tau = g.cond_tau;
   a.flag_or = g.flag_or;
+  a.tri = g.tri;
   return g.fp64 ? launch_pf_d<double>(a, g.d, st) : launch_pf_d<float>(a, g.d, st);
 }
 
