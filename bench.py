@@ -16,7 +16,8 @@ chosen form (tcgen05 BF16x3 CNN, learned hop proposal with the exact Hastings co
 trained on 2^20 records of the plain chains): acceptance, tau_int of the log|psi| series,
 effective samples per second and the energy per site of each, on 1024 chains that start from
 the same configurations after 6000 equilibration steps.  ``local_energy`` (1 GPU) times the
-ragged local energy of 4096 configurations at 8x8 and 16x16, one CUDA-graph replay each.
+ragged local energy at 8x8, 16x16 and 24x24, one CUDA-graph replay each; ``large_lattice``
+(1 GPU) times Metropolis steps at 32x32 (n = 896) with the uniform hop and the learned proposal.
 ``precision`` (1 GPU) reports each precision form's |delta log|psi_P|| and sign mismatches
 against the library's all-FP64 path, and near-nodal log-Pfaffians at the slogpf boundary.
 
@@ -293,6 +294,7 @@ def measure_sampling(args, dev, st, seed) -> dict:
                      "energy_per_site_err": float(e.std(ddof=1) / np.sqrt(ne))}
         del smp
     out["chosen"]["proposal_training"] = train
+    out["_proposal"] = q
     d = out["chosen"]["energy_per_site"] - out["plain"]["energy_per_site"]
     sig = float(np.hypot(out["chosen"]["energy_per_site_err"], out["plain"]["energy_per_site_err"]))
     out["energy_difference_sigma"] = abs(d) / sig if sig > 0 else None
@@ -320,14 +322,14 @@ def measure_local_energy(args, dev, st) -> dict:
 
     out = {}
     H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2])
-    for Lk, cnn_mode in ((8, 0), (16, 0), (16, 2)):
+    for Lk, cnn_mode in ((8, 0), (16, 0), (16, 2), (24, 0)):
         Nk = Lk * Lk
         nek = 7 * Nk // 16
         params = nh.init_params(Lk, Lk, CHANNELS, LAYERS, std=0.02, seed=0)
         model = nh.PfaffianBackflow(Lk, Lk, nek, nek, params=params, device=dev,
                                     cnn_mode=cnn_mode)
         state = nh.Variational(model, symm=False, max_parallel=8192)
-        B = args.eloc_samples
+        B = args.eloc_samples if Lk <= 16 else min(args.eloc_samples, 256)
         spins = torch.from_numpy(nh.random_spins(np.random.default_rng(500 + Lk), B, Nk, nek,
                                                  nek)).to(dev)
         psi = state(spins)
@@ -362,9 +364,9 @@ def measure_local_energy(args, dev, st) -> dict:
             "energy_per_site_err": float(ev.std(ddof=1) / np.sqrt(B))}
         del graph, e, state, model
         torch.cuda.empty_cache()
-    out["setup"] = ("4096 uniformly random configurations per lattice, unprojected amplitudes, "
-                    "t = 1, t' = -0.2, U = 8; one CUDA-graph replay of the whole call; "
-                    "24x24 (n = 504) exceeds the shared-memory Pfaffian (n <= 256)")
+    out["setup"] = ("4096 uniformly random configurations at 8x8 and 16x16, 256 at 24x24 (n = "
+                    "504, large-lattice path: 40 ms of amplitudes per sample), unprojected "
+                    "amplitudes, t = 1, t' = -0.2, U = 8; one CUDA-graph replay of the whole call")
     return out
 
 
@@ -448,6 +450,62 @@ def measure_precision(dev, st, spins, flush) -> dict:
     torch.cuda.empty_cache()
     out["reference"] = ("all-FP64 path of the library (FP64 CNN, gather and Pfaffian), which "
                         "matches the numpy oracle to 1e-9 in the parity tests")
+    return out
+
+
+def measure_large(args, dev, st, q) -> dict:
+    """Config 5 shapes: Metropolis at 32x32 (n = 896, large-lattice path) with 4096 chains x 8
+    images, uniform hop against the learned proposal (the 16x16-trained weights: the proposal
+    network is translation-equivariant); one untimed and ``large_steps`` timed steps each."""
+    import torch
+
+    import neuralhubbard_b200 as nh
+
+    Lk, B = 32, args.large_chains
+    Nk = Lk * Lk
+    nek = 7 * Nk // 16
+    params = nh.init_params(Lk, Lk, CHANNELS, LAYERS, std=0.02, seed=0)
+    model = nh.PfaffianBackflow(Lk, Lk, nek, nek, params=params, device=dev)
+    state = nh.Variational(model, symm=True, max_parallel=8192)
+    init = nh.random_spins(np.random.default_rng(31), B, Nk, nek, nek)
+    out = {"lattice": "32x32", "pfaffian_n": 2 * nek, "chains": B, "images": IMAGES,
+           "timed_steps": args.large_steps}
+    q32 = None
+    if q is not None:
+        q32 = nh.HopProposal(Lk, Lk, 8, params=q.numpy(), device=dev)
+    for name, make in (("uniform_hop", lambda: nh.ParticleHop(state, B, n_neighbor=(1, 2),
+                                                              initial_spins=init, seed=32)),
+                       ("learned", lambda: nh.LearnedHop(state, B, q32, initial_spins=init,
+                                                         seed=33) if q32 else None)):
+        smp = make()
+        if smp is None:
+            continue
+        smp.run(1)
+        a0 = int(smp.accepted.sum().item())
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        smp.run(args.large_steps)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.large_steps
+        out[name] = {"ms_per_step": ms,
+                     "acceptance": (int(smp.accepted.sum().item()) - a0) / (B * args.large_steps)}
+        del smp
+    t = torch.from_numpy(init[:512]).to(dev)
+    state(t)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    state(t)
+    e1.record(st)
+    torch.cuda.synchronize()
+    out["amplitudes_per_s"] = 512 * IMAGES / (e0.elapsed_time(e1) / 1e3)
+    out["note"] = ("tau_int is not measured at 32x32 within the bench (about 2.4 s per step with "
+                   "4096 chains); the proposal is trained at 16x16 (its backward kernel holds "
+                   "the activations of up to 559 sites in shared memory) and transferred")
     return out
 
 
@@ -553,8 +611,13 @@ def run_ours(args) -> None:
     kernels = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1]} for k, v in kern.items()}
 
     sampling = None
+    q16 = None
     if world == 1 and not args.no_sampling:
         sampling = measure_sampling(args, dev, st, seed=77)
+        q16 = sampling.pop("_proposal")
+    large = None
+    if world == 1 and not args.no_large:
+        large = measure_large(args, dev, st, q16)
     local_energy = None
     if world == 1 and not args.no_eloc:
         local_energy = measure_local_energy(args, dev, st)
@@ -585,6 +648,7 @@ def run_ours(args) -> None:
                     "d2h_bytes_per_step": BATCH * (4 + 8)},
             "sampling": sampling,
             "local_energy": local_energy,
+            "large_lattice": large,
             "precision": precision,
             "roofline": roof, "kernels": kernels, "gpu_launches": launches,
             "cpu_baseline": cpu, "clocks": clk,
@@ -639,6 +703,10 @@ def main():
     ap.add_argument("--no-eloc", action="store_true",
                     help="skip the ragged local-energy measurement (8x8 and 16x16)")
     ap.add_argument("--eloc-samples", type=int, default=4096)
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the 32x32 (n = 896) Metropolis measurement")
+    ap.add_argument("--large-chains", type=int, default=4096)
+    ap.add_argument("--large-steps", type=int, default=2)
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the precision-form report (errors against the all-FP64 path)")
     ap.add_argument("--chains", type=int, default=1024)
