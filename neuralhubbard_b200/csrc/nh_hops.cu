@@ -168,9 +168,26 @@ __global__ void eloc_reduce_kernel(const int8_t* __restrict__ spins, const float
     double acc = 0.0;
     const double l0 = logabs[b];
     const float s0 = sign[b];
-    for (int64_t c = offsets[b] + lane; c < offsets[b + 1]; c += 32) {
+    const int64_t c1 = offsets[b + 1];
+    int64_t c = offsets[b] + lane;
+    // Four connections per lane per pass, all loads issued before any is used.
+    for (; c + 96 < c1; c += 128) {
+      float sc[4];
+      double hv[4], la[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        sc[u] = csign[c + 32 * u];
+        hv[u] = hval[c + 32 * u];
+        la[u] = clogabs[c + 32 * u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (sc[u] != 0.0f) acc += hv[u] * (double)(sc[u] * s0) * exp(la[u] - l0);
+    }
+    for (; c < c1; c += 32) {
       const float sc = csign[c];
-      if (sc != 0.0f) acc += hval[c] * (double)(sc * s0) * exp(clogabs[c] - l0);
+      const double hv = hval[c], la = clogabs[c];
+      if (sc != 0.0f) acc += hv * (double)(sc * s0) * exp(la - l0);
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) {

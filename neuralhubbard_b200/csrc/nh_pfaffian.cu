@@ -519,6 +519,105 @@ __global__ void __launch_bounds__(kNumThreads) pairing_kernel(const float* __res
   }
 }
 
+// Shared-memory variant: the Wt table is staged once per CTA and each matrix's occupied features
+// once per matrix, rows padded to D + 4 floats (16-byte chunks of 8 consecutive rows fall in
+// distinct banks); a warp computes two rows per pass so that each feature row it loads serves
+// two outputs.  Same per-element arithmetic as pair_value: F is bit-for-bit that of the fused
+// gather and exactly antisymmetric.
+template <int D>
+__global__ void __launch_bounds__(kNumThreads) pairing_smem_kernel(
+    const float* __restrict__ Y, const int32_t* __restrict__ idx, const float* __restrict__ Wt,
+    int Lx, int Ly, int n, int batch, float* __restrict__ F) {
+  constexpr int DP = D + 4;
+  extern __shared__ __align__(16) float psm[];
+  const int N = Lx * Ly;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  float* wts = psm;            // (4 N, DP)
+  float* ys = wts + 4 * N * DP;  // (n, DP)
+  int* info = reinterpret_cast<int*>(ys + n * DP);  // (spin << 16) | (x << 8) | y per row
+  for (int e = tid; e < 4 * N * D; e += kNumThreads) {
+    const int row = e / D;
+    wts[row * DP + (e - row * D)] = __ldg(Wt + e);
+  }
+  for (int item = blockIdx.x; item < batch; item += gridDim.x) {
+    const float* Yi = Y + (size_t)item * n * D;
+    const int32_t* ii = idx + (size_t)item * n;
+    float* Fi = F + (size_t)item * n * n;
+    __syncthreads();
+    for (int e = tid; e < n * D; e += kNumThreads) {
+      const int row = e / D;
+      ys[row * DP + (e - row * D)] = __ldg(Yi + e);
+    }
+    for (int p = tid; p < n; p += kNumThreads) {
+      const int m = __ldg(ii + p);
+      const int sp = m >= N ? 1 : 0;
+      const int site = m - sp * N;
+      const int x = site / Ly;
+      info[p] = (sp << 16) | (x << 8) | (site - x * Ly);
+    }
+    __syncthreads();
+    for (int p0 = 2 * wid; p0 < n; p0 += 2 * kWarps) {
+      const int np = p0 + 1 < n ? 2 : 1;
+      float yp[2][D];
+      int sp[2], xp[2], ypos[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int p = h < np ? p0 + h : p0;
+#pragma unroll
+        for (int a0 = 0; a0 < D; a0 += 4) {
+          const float4 v = *reinterpret_cast<const float4*>(ys + p * DP + a0);
+          yp[h][a0] = v.x;
+          yp[h][a0 + 1] = v.y;
+          yp[h][a0 + 2] = v.z;
+          yp[h][a0 + 3] = v.w;
+        }
+        const int inf = info[p];
+        sp[h] = inf >> 16;
+        xp[h] = (inf >> 8) & 0xFF;
+        ypos[h] = inf & 0xFF;
+      }
+      for (int q = lane; q < n; q += 32) {
+        float yq[D];
+#pragma unroll
+        for (int a0 = 0; a0 < D; a0 += 4) {
+          const float4 v = *reinterpret_cast<const float4*>(ys + q * DP + a0);
+          yq[a0] = v.x;
+          yq[a0 + 1] = v.y;
+          yq[a0 + 2] = v.z;
+          yq[a0 + 3] = v.w;
+        }
+        const int inf = info[q];
+        const int sq = inf >> 16, xq = (inf >> 8) & 0xFF, yqp = inf & 0xFF;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (h >= np) continue;
+          const int p = p0 + h;
+          float acc = 0.0f;
+          if (q != p) {
+            int dx = xp[h] - xq, dy = ypos[h] - yqp;
+            dx += dx < 0 ? Lx : 0;
+            dy += dy < 0 ? Ly : 0;
+            const float* w = wts + ((2 * sp[h] + sq) * N + dx * Ly + dy) * DP;
+#pragma unroll
+            for (int a0 = 0; a0 < D; a0 += 4) {
+              const float4 wv = *reinterpret_cast<const float4*>(w + a0);
+              acc = fmaf(yp[h][a0] * yq[a0], wv.x, acc);
+              acc = fmaf(yp[h][a0 + 1] * yq[a0 + 1], wv.y, acc);
+              acc = fmaf(yp[h][a0 + 2] * yq[a0 + 2], wv.z, acc);
+              acc = fmaf(yp[h][a0 + 3] * yq[a0 + 3], wv.w, acc);
+            }
+          }
+          Fi[(size_t)p * n + q] = acc;
+        }
+      }
+    }
+  }
+}
+
+size_t pairing_smem_bytes(int N, int n, int D) {
+  return sizeof(float) * (4 * (size_t)N + n) * (D + 4) + sizeof(int) * (size_t)n;
+}
+
 // ------------------------------------------------------------------ image combination
 // Also used with G = 1 to copy the per-item results into the caller's arrays.
 // Sum over the images of one configuration in FP64: returns sum_g s_g exp(l_g - m) and sets
@@ -1101,9 +1200,35 @@ int launch_pfaffian_tc(const PfGatherArgs& g, int mode, const float* F, int32_t*
   }
 }
 
+template <int D>
+int launch_pairing_smem(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int n,
+                        int batch, float* F, size_t smem, cudaStream_t st) {
+  static size_t configured = 0;
+  if (smem > 48 * 1024 && smem > configured) {
+    cudaError_t e = cudaFuncSetAttribute(pairing_smem_kernel<D>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return check_cuda(e, "pairing smem attribute");
+    configured = smem;
+  }
+  int grid = num_sms() * (smem <= 113 * 1024 ? 2 : 1);
+  if (grid > batch) grid = batch;
+  ProfScope prof_scope(NH_K_PAIRING, st);
+  pairing_smem_kernel<D><<<grid, kNumThreads, smem, st>>>(Y, idx, Wt, Lx, Ly, n, batch, F);
+  return check_launch("pairing_smem_kernel");
+}
+
 int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
                    int n, int batch, float* F, cudaStream_t st) {
   if (batch <= 0) return NH_OK;
+  const size_t smem = pairing_smem_bytes(Lx * Ly, n, d);
+  if (smem <= 227 * 1024 && Lx < 256 && Ly < 256) {
+    switch (d) {
+      case 8: return launch_pairing_smem<8>(Y, idx, Wt, Lx, Ly, n, batch, F, smem, st);
+      case 16: return launch_pairing_smem<16>(Y, idx, Wt, Lx, Ly, n, batch, F, smem, st);
+      case 32: return launch_pairing_smem<32>(Y, idx, Wt, Lx, Ly, n, batch, F, smem, st);
+      default: break;
+    }
+  }
   int grid = num_sms() * 4;
   if (grid > batch) grid = batch;
   ProfScope prof_scope(NH_K_PAIRING, st);
