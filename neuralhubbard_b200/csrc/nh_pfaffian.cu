@@ -646,11 +646,14 @@ __device__ __forceinline__ double image_sum(const float* __restrict__ sg,
   return tot;
 }
 
-// Recompute selection for projected amplitudes, before the FP64 list is built: every image of a
-// configuration whose images cancel (sum |.| > cancel_tau |sum|, cancel_tau > 0) is marked; an
-// ill-conditioned image (NH_FLAG_GROWTH) whose share |psi_g| / |sum_g eta_g psi_g| is below
-// kImageWeightFloor is unmarked, since even a 1e-2 error in it moves log|psi_P| by < 1e-5.
+// Recompute selection for projected amplitudes, before the FP64 list is built.  An image's
+// error reaches log|psi_P| weighted by w_g = |psi_g| / |sum_g eta_g psi_g|.  In a configuration
+// whose images cancel (sum |.| > cancel_tau |sum|, cancel_tau > 0) the images with
+// w_g > kCancelImageFloor are marked: an FP32 image error (at most ~1e-3) of the others adds
+// < 2e-5.  An ill-conditioned image (NH_FLAG_GROWTH) with w_g < kImageWeightFloor is unmarked:
+// even a 1e-2 error in it moves log|psi_P| by < 1e-5.
 constexpr double kImageWeightFloor = 1e-3;
+constexpr double kCancelImageFloor = 2e-2;
 
 __global__ void image_mark_kernel(const float* __restrict__ sg, const double* __restrict__ la,
                                   int32_t* __restrict__ fl, int G, int n_cfg,
@@ -660,7 +663,11 @@ __global__ void image_mark_kernel(const float* __restrict__ sg, const double* __
     double m, a;
     const double tot = image_sum(sg, la, c, G, &m, &a);
     if (cancel_tau > 0.0 && a > 0.0 && a > cancel_tau * fabs(tot)) {
-      for (int g = 0; g < G; ++g) fl[(size_t)c * G + g] |= NH_FLAG_GROWTH | NH_FLAG_CANCEL;
+      for (int g = 0; g < G; ++g) {
+        const size_t i = (size_t)c * G + g;
+        if (sg[i] != 0.0f && exp(la[i] - m) > kCancelImageFloor * fabs(tot))
+          fl[i] |= NH_FLAG_GROWTH | NH_FLAG_CANCEL;
+      }
     } else if (prune && tot != 0.0) {
       for (int g = 0; g < G; ++g) {
         const size_t i = (size_t)c * G + g;

@@ -424,9 +424,9 @@ def test_local_energy_chunk_autotune():
 
 
 def test_cancellation_recompute():
-    """cancel_tau: configurations whose 8 images cancel are recomputed in FP64 image by image;
-    their projected amplitude then equals the all-FP64 result bit for bit, and no configuration
-    is worse than without the recompute."""
+    """cancel_tau: in configurations whose 8 images cancel, the images carrying more than 2% of
+    |psi_P| are recomputed in FP64; those configurations then agree with the all-FP64 result to
+    1e-4 (the FP32 images left carry < 2% weight), the others are unchanged."""
     L, ne = 16, 112
     params = nh.init_params(L, L, channels=32, std=0.02, seed=0)
     s = torch.from_numpy(nh.random_spins(np.random.default_rng(1000), 512, L * L, ne, ne)).to(DEV)
@@ -441,8 +441,9 @@ def test_cancellation_recompute():
     assert 0 < cancel.sum() < len(fl)
     assert np.all(fl[cancel] & _lib.FLAG_REFINED)
     la, l0, lb = psi.logabs.cpu().numpy(), ref.logabs.cpu().numpy(), base.logabs.cpu().numpy()
-    assert np.array_equal(la[cancel], l0[cancel])
+    assert np.max(np.abs(la[cancel] - l0[cancel])) < 1e-4
+    assert np.array_equal(la[~cancel], lb[~cancel])
     assert torch.equal(psi.sign, ref.sign)
-    assert np.all(np.abs(la - l0) <= np.abs(lb - l0) + 1e-12)
+    assert np.abs(la - l0).max() <= np.abs(lb - l0).max()
     # the flag reports the cancellation factor of the final amplitude
     assert not (base.flags.cpu().numpy() & _lib.FLAG_CANCEL).any()
