@@ -65,8 +65,7 @@ enum {
  * Wt64:          the same table in FP64 (nh_build_wtilde), or null to disable the FP64
  *                recompute of ill-conditioned items.
  * cond_tau:      an item whose largest / smallest pivot magnitude exceeds cond_tau is flagged
- *                NH_FLAG_GROWTH and, when Wt64 is set and the FP64 kernels fit in shared
- *                memory (n <= 232, N <= 256 at 32 channels), recomputed end to end in FP64
+ *                NH_FLAG_GROWTH and, when Wt64 is set, recomputed end to end in FP64
  *                (CNN, gather, Pfaffian; NH_FLAG_REFINED); <= 0 disables both.  For projected
  *                amplitudes with cond_tau > 1 an image whose |psi(g s)| is below 1e-3 of
  *                |psi_P(s)| is not recomputed (its error cannot move log|psi_P| by more than
@@ -181,7 +180,10 @@ int nh_slogpf_noalloc(const float* F, int n, int batch, double cond_tau, float* 
                       double* logabs, int32_t* flags, void* stream);
 
 /* Amplitudes of batch configurations.  n_symm = 1: psi(s); n_symm = 8: the projection onto the
- * trivial representation of Flip(0) Flip(1) SpinInverse, psi_P(s) = 1/8 sum_g eta_g psi(g s). */
+ * trivial representation of Flip(0) Flip(1) SpinInverse, psi_P(s) = 1/8 sum_g eta_g psi(g s).
+ * Lattices up to 32 x 32 and n = n_up + n_dn <= 1024: beyond n = 256 (FP32) / 232 (FP64) the
+ * Pfaffian keeps its triangles, and beyond shared memory the CNN its activation planes, in a
+ * per-CTA scratch that the workspace query includes (e.g. ~0.4 GB at 32 x 32). */
 size_t nh_amplitude_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p);
 int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_params* p,
                  float* sign, double* logabs, int32_t* flags, void* workspace,

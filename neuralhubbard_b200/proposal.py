@@ -118,8 +118,7 @@ class HopProposal:
                   float(beta1), float(beta2), float(eps), self.weights.data_ptr(),
                   stream_ptr(self.device))
 
-    def train(self, records, steps: int, batch: int = 512, lr: float = 3e-3, seed: int = 0,
-              log_every: int = 0):
+    def train(self, records, steps: int, batch: int = 512, lr: float = 3e-3, seed: int = 0):
         """Adam on minibatches drawn (seeded, with replacement across epochs) from ``records``
         = (spins, moves, weights).  Returns the per-step losses (host floats)."""
         spins, moves, weights = records
