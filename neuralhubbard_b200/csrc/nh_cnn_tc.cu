@@ -14,7 +14,12 @@
 // accumulates hi*hi + hi*lo + lo*hi (about 16 significant bits per product) for near-FP32
 // features.  The layer-0 input (+-1 occupations) is exact in BF16.  Bias, GELU and the split run
 // in FP32 in the epilogue, which reads the accumulators with tcgen05.ld (warp w % 4 owns lanes
-// 32 (w % 4) .. + 31, warps 0-3 read tile 0 and warps 4-7 tile 1).
+// 32 (w % 4) .. + 31 of both tiles).
+//
+// Two warp groups of 128 threads run independent image streams in one CTA: each has its own
+// activation planes, bookkeeping, mbarrier, 64 tensor-memory columns and named barrier, and
+// shares the resident weights; while one group's MMAs run, the other converts its accumulators
+// (bias, GELU, hi/lo split) and writes its next planes.
 //
 // Output: the occupied rows Y (n, d) FP32 of the image configuration, the occupied-mode list and
 // the item sign, like the CUDA-core kernel (mode 1 of nh_cnn.cu).
@@ -41,7 +46,10 @@ constexpr int kW0Bytes = 2 * 9 * 2 * 4 * 128;    // layer 0: q x tap x kc(2) x c
 constexpr int kW1Bytes = 2 * 9 * 4 * 4 * 128;    // layers 1..3: q x tap x kc(4) x cg(4) x 128 B
 constexpr int kWBytes = kW0Bytes + 3 * kW1Bytes;
 constexpr int kActBytes = 2 * 4 * kPlane;        // hi and lo, 4 planes each
-constexpr unsigned kTmemCols = 64;               // two 128 x 32 FP32 accumulators
+constexpr int kWG = 2;                           // independent warp groups per CTA
+constexpr int kWGThreads = kTcThreads / kWG;     // 128
+constexpr int kIntsPerWG = 3 * 2 * kL * kL + 4 * kL + 32;  // simg, rowof, occl, scan scratch
+constexpr unsigned kTmemCols = 64 * kWG;         // two 128 x 32 FP32 accumulators per group
 constexpr long long kWaitLimit = 1ll << 22;      // mbarrier polls before giving up
 
 struct TcArgs {
@@ -187,20 +195,49 @@ __device__ void issue_layer(uint32_t tmem, uint32_t act_hi, uint32_t act_lo, uin
   }
 }
 
+__device__ __forceinline__ void wg_sync(int wg) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + wg), "r"(kWGThreads) : "memory");
+}
+
+struct WgSync {
+  int wg;
+  __device__ void operator()() const { wg_sync(wg); }
+};
+
+// Convert one 128 x 32 accumulator tile row (32 channels of one site) of layers 0-2 into the
+// next layer's BF16 hi / lo 8-channel groups.
+__device__ __forceinline__ void act_groups(const float* v, const float* bl, uint4* hi,
+                                           uint4* lo) {
+#pragma unroll
+  for (int kc = 0; kc < 4; ++kc) {
+    uint32_t ph[4], pl[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float f0 = gelu_tanh(v[8 * kc + 2 * j] + bl[8 * kc + 2 * j]);
+      const float f1 = gelu_tanh(v[8 * kc + 2 * j + 1] + bl[8 * kc + 2 * j + 1]);
+      const uint16_t h0 = bf16_bits(f0), h1 = bf16_bits(f1);
+      ph[j] = (uint32_t)h0 | ((uint32_t)h1 << 16);
+      pl[j] = (uint32_t)bf16_bits(f0 - bf16_val(h0)) |
+              ((uint32_t)bf16_bits(f1 - bf16_val(h1)) << 16);
+    }
+    hi[kc] = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+    lo[kc] = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+  }
+}
+
 __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  unsigned char* wsm = smem;                 // packed weights (kWBytes)
-  unsigned char* act = smem + kWBytes;       // [q][kc] planes (kActBytes)
-  float* bsm = reinterpret_cast<float*>(act + kActBytes);  // (4, 32) biases
-  int* simg = reinterpret_cast<int*>(bsm + 4 * kC);         // (2N) image configuration
-  int* rowof = simg + 2 * kL * kL;                          // (2N) mode -> row of Y, or -1
-  int* occl = rowof + 2 * kL * kL;                          // (2N) ascending occupied modes
-  int* wbuf = occl + 2 * kL * kL;                           // (4 L + 32) scan scratch
-  uint64_t* bar = reinterpret_cast<uint64_t*>(wbuf + 4 * kL + 32);  // mbarrier
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
-  int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+  unsigned char* wsm = smem;                             // packed weights (kWBytes)
+  unsigned char* act_all = smem + kWBytes;               // per group: [q][kc] planes
+  float* bsm = reinterpret_cast<float*>(act_all + kWG * kActBytes);  // (4, 32) biases
+  int* ints_all = reinterpret_cast<int*>(bsm + 4 * kC);  // per group: kIntsPerWG
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ints_all + kWG * kIntsPerWG);  // per group
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kWG);
+  int* abort_all = reinterpret_cast<int*>(tmem_slot + 1);  // per group
 
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tid = threadIdx.x;
+  const int wg = tid / kWGThreads, ltid = tid - wg * kWGThreads;
+  const int lane = ltid & 31, lwid = ltid >> 5;  // lwid = warp % 4: the TMEM lane quarter
   const int N = kL * kL, M2 = 2 * N;
 
   // Weights and biases resident for the whole launch.
@@ -208,11 +245,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
     reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.wpk) + i);
   for (int i = tid; i < 4 * kC; i += kTcThreads) bsm[i] = __ldg(a.bias + i);
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    for (int w = 0; w < kWG; ++w) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars + w)) : "memory");
+      abort_all[w] = 0;
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    *abort_flag = 0;
   }
-  if (wid == 0) {
+  if (tid < 32) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
                  "r"(kTmemCols)
@@ -222,7 +261,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t tmem = *tmem_slot;
+
+  // This warp group's state.
+  const uint32_t tmem = *tmem_slot + 64u * wg;
+  unsigned char* act = act_all + wg * kActBytes;
+  int* simg = ints_all + wg * kIntsPerWG;  // (2N) image configuration
+  int* rowof = simg + M2;                  // (2N) mode -> row of Y, or -1
+  int* occl = rowof + M2;                  // (2N) ascending occupied modes
+  int* wbuf = occl + M2;                   // (4 L + 32) scan scratch
+  uint64_t* bar = bars + wg;
+  int* abort_flag = abort_all + wg;
   const uint32_t act_hi = smem_u32(act), act_lo = act_hi + 4 * kPlane;
   const uint32_t w0 = smem_u32(wsm);
   const bool split = a.mode == 2;
@@ -230,9 +278,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
 
   const int G = a.cl.G;
   const int n_items = (a.cl.n_cfg_dev ? *a.cl.n_cfg_dev : a.cl.n_cfg) * G;
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+  for (int item = blockIdx.x * kWG + wg; item < n_items; item += gridDim.x * kWG) {
     if (*abort_flag) {  // a wait expired earlier: mark the item instead of computing it
-      if (tid == 0) a.item_sign[item] = NAN;
+      if (ltid == 0) a.item_sign[item] = NAN;
       continue;
     }
     const int c = item / G, g = item - c * G;
@@ -240,16 +288,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
     const int fr = a.cl.from ? a.cl.from[c] : -1;
     const int to = a.cl.from ? a.cl.to[c] : -1;
     const int8_t* base = a.cl.spins + (int64_t)smp * M2;
-    __syncthreads();
-    for (int m = tid; m < M2; m += kTcThreads) {
+    wg_sync(wg);
+    for (int m = ltid; m < M2; m += kWGThreads) {
       const int src = sym_map(m, g, kL, kL, N);
       int v = base[src];
       v = (src == fr) ? -1 : ((src == to) ? 1 : v);
       simg[m] = v > 0 ? 1 : -1;
     }
-    __syncthreads();
+    wg_sync(wg);
     // Layer-0 input planes: channel 0 = up, 1 = down (+-1, exact in BF16), the rest zero.
-    for (int s = tid; s < N; s += kTcThreads) {
+    for (int s = ltid; s < N; s += kWGThreads) {
       uint4 grp[2];
       const uint32_t up = bf16_bits((float)simg[s]), dn = bf16_bits((float)simg[N + s]);
       grp[0] = make_uint4(up | (dn << 16), 0u, 0u, 0u);
@@ -258,8 +306,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
     }
     // Occupied modes of the image configuration (ascending) and their rows in Y.
     {
-      const int per = (M2 + kTcThreads - 1) / kTcThreads;
-      const int m0 = tid * per;
+      const int per = (M2 + kWGThreads - 1) / kWGThreads;
+      const int m0 = ltid * per;
       int cnt = 0;
       for (int m = m0; m < m0 + per && m < M2; ++m) cnt += simg[m] > 0;
       int x = cnt;
@@ -268,11 +316,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
         const int y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
       }
-      if (lane == 31) wbuf[wid] = x;
-      __syncthreads();
+      if (lane == 31) wbuf[lwid] = x;
+      wg_sync(wg);
       int before = 0, total = 0;
-      for (int w = 0; w < kTcThreads / 32; ++w) {
-        before += w < wid ? wbuf[w] : 0;
+      for (int w = 0; w < kWGThreads / 32; ++w) {
+        before += w < lwid ? wbuf[w] : 0;
         total += wbuf[w];
       }
       int pos = before + x - cnt;
@@ -285,15 +333,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
           rowof[m] = -1;
         }
       }
-      __syncthreads();
-      if (tid == 0) wbuf[0] = total;
+      wg_sync(wg);
+      if (ltid == 0) wbuf[0] = total;
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
+    wg_sync(wg);
     const int total = wbuf[0];
 
     for (int layer = 0; layer < 4; ++layer) {
-      if (tid == 0) {
+      if (ltid == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (layer == 0)
           issue_layer(tmem, act_hi, act_lo, w0, w0 + kW0Bytes / 2, 2, 2 * 4 * 128, false, split);
@@ -304,70 +352,68 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
         mma_commit(bar);
       }
       if (!mbar_wait(bar, phase)) {
-        if (tid == 0) atomicExch(a.err, 1);
+        if (ltid == 0) atomicExch(a.err, 1);
         *abort_flag = 1;
       }
       phase ^= 1u;
-      __syncthreads();
+      wg_sync(wg);
       if (*abort_flag) {
-        if (tid == 0) a.item_sign[item] = NAN;
+        if (ltid == 0) a.item_sign[item] = NAN;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 of tile w / 4.
-      const int h = wid >> 2, sub = wid & 3;
-      float v[32];
-      tmem_ld32(tmem + ((uint32_t)(32 * sub) << 16) + 32 * h, v);
-      const int mrow = 32 * sub + lane;            // row of the 128 x 32 tile
-      const int x = mrow >> 3, y = 8 * h + (mrow & 7);
+      // Epilogue: warp lwid reads TMEM lanes 32 lwid .. + 31 of both tiles (rows = sites).
+      const int mrow = 32 * lwid + lane;  // row of the 128 x 32 tile
+      const int x = mrow >> 3;
       const float* bl = bsm + layer * kC;
       if (layer < 3) {
-        uint4 hi[4], lo[4];
+        uint4 hi[2][4], lo[2][4];
 #pragma unroll
-        for (int kc = 0; kc < 4; ++kc) {
-          uint32_t ph[4], pl[4];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const float f0 = gelu_tanh(v[8 * kc + 2 * j] + bl[8 * kc + 2 * j]);
-            const float f1 = gelu_tanh(v[8 * kc + 2 * j + 1] + bl[8 * kc + 2 * j + 1]);
-            const uint16_t h0 = bf16_bits(f0), h1 = bf16_bits(f1);
-            ph[j] = (uint32_t)h0 | ((uint32_t)h1 << 16);
-            pl[j] = (uint32_t)bf16_bits(f0 - bf16_val(h0)) |
-                    ((uint32_t)bf16_bits(f1 - bf16_val(h1)) << 16);
-          }
-          hi[kc] = make_uint4(ph[0], ph[1], ph[2], ph[3]);
-          lo[kc] = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+        for (int h = 0; h < 2; ++h) {
+          float v[32];
+          tmem_ld32(tmem + ((uint32_t)(32 * lwid) << 16) + 32 * h, v);
+          act_groups(v, bl, hi[h], lo[h]);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();  // every tile is read before any plane is overwritten
-        put_site(act, 4, x, y, hi);
-        if (split) put_site(act + 4 * kPlane, 4, x, y, lo);
+        wg_sync(wg);  // every tile is read before any plane is overwritten
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int y = 8 * h + (mrow & 7);
+          put_site(act, 4, x, y, hi[h]);
+          if (split) put_site(act + 4 * kPlane, 4, x, y, lo[h]);
+        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
+        wg_sync(wg);
       } else {
         // Last layer: features y_up = channels 0..15, y_down = 16..31 of occupied modes.
-        const int s = x * kL + y;
 #pragma unroll
-        for (int sg = 0; sg < 2; ++sg) {
-          const int row = rowof[sg * N + s];
-          if (row < 0) continue;
-          float4* dst = reinterpret_cast<float4*>(a.Y + ((int64_t)item * a.n + row) * 16);
+        for (int h = 0; h < 2; ++h) {
+          float v[32];
+          tmem_ld32(tmem + ((uint32_t)(32 * lwid) << 16) + 32 * h, v);
+          const int s = x * kL + 8 * h + (mrow & 7);
 #pragma unroll
-          for (int q = 0; q < 4; ++q)
-            dst[q] = make_float4(v[16 * sg + 4 * q] + bl[16 * sg + 4 * q],
-                                 v[16 * sg + 4 * q + 1] + bl[16 * sg + 4 * q + 1],
-                                 v[16 * sg + 4 * q + 2] + bl[16 * sg + 4 * q + 2],
-                                 v[16 * sg + 4 * q + 3] + bl[16 * sg + 4 * q + 3]);
+          for (int sg = 0; sg < 2; ++sg) {
+            const int row = rowof[sg * N + s];
+            if (row < 0) continue;
+            float4* dst = reinterpret_cast<float4*>(a.Y + ((int64_t)item * a.n + row) * 16);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              dst[q] = make_float4(v[16 * sg + 4 * q] + bl[16 * sg + 4 * q],
+                                   v[16 * sg + 4 * q + 1] + bl[16 * sg + 4 * q + 1],
+                                   v[16 * sg + 4 * q + 2] + bl[16 * sg + 4 * q + 2],
+                                   v[16 * sg + 4 * q + 3] + bl[16 * sg + 4 * q + 3]);
+          }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       }
     }
     if (*abort_flag) continue;
     // Occupied-mode list and item sign (eta_g times the descending-order convention).
-    for (int p = tid; p < a.n; p += kTcThreads)
+    for (int p = ltid; p < a.n; p += kWGThreads)
       a.idx[(int64_t)item * a.n + p] = occl[p < total ? p : 0];
-    const int odd = image_sign_parity(simg, g, kL, kL, wbuf);
-    if (tid == 0) {
+    const int odd = image_sign_parity_group(simg, g, kL, kL, wbuf, ltid, kWGThreads / 32,
+                                            WgSync{wg});
+    if (ltid == 0) {
       const long long kk = total;
       const int rev = (int)((kk * (kk - 1) / 2) & 1);
       float sgn = ((odd & 1) ^ rev) ? -1.0f : 1.0f;
@@ -377,8 +423,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (wid == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+  if (tid < 32)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot),
                  "r"(kTmemCols)
                  : "memory");
 }
@@ -420,8 +466,9 @@ __global__ void pack_tc_kernel(const float* __restrict__ w, uint16_t* out) {
   }
 }
 
-constexpr size_t kTcSmem = (size_t)kWBytes + kActBytes + 4 * kC * sizeof(float) +
-                           sizeof(int) * (3 * 2 * kL * kL + 4 * kL + 32) + 64;
+constexpr size_t kTcSmem = (size_t)kWBytes + kWG * kActBytes + 4 * kC * sizeof(float) +
+                           sizeof(int) * kWG * kIntsPerWG + 64;
+static_assert(kTcSmem <= 227 * 1024, "two warp groups must fit in shared memory");
 
 }  // namespace
 
@@ -453,7 +500,7 @@ int launch_cnn_tc(const ConfigList& cl, const nh_backflow_params& p, int mode, f
   const int items = cl.n_cfg * cl.G;
   if (items <= 0) return NH_OK;
   int grid = num_sms();
-  if (grid > items) grid = items;
+  if (grid > (items + kWG - 1) / kWG) grid = (items + kWG - 1) / kWG;
   TcArgs a{cl, static_cast<const uint16_t*>(p.conv_w_tc), p.conv_b, p.n_up + p.n_dn, mode, Y,
            idx, item_sign, err};
   ProfScope prof_scope(NH_K_CNN_TC, st);

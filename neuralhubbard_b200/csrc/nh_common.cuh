@@ -50,9 +50,12 @@ __host__ __device__ __forceinline__ int hop_target_site(int site, int dir, int L
 // x-flip inverts every pair of occupied sites in distinct rows x1, x2 >= 1, y-flip every pair in
 // one row with y1, y2 >= 1, the spin swap every (up, down) pair.  Block-wide (all threads call
 // it); scratch holds 4 Lx + 4 ints.  Lx <= 32 rows, Ly <= 32 sites per row.
-__device__ __forceinline__ int image_sign_parity(const int* simg, int g, int Lx, int Ly,
-                                                 int* scratch) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// Generic form over a group of threads: local thread index ltid, nw warps, and the group's
+// barrier (the block barrier below; a named warp-group barrier in the tensor-core CNN).
+template <typename Sync>
+__device__ __forceinline__ int image_sign_parity_group(const int* simg, int g, int Lx, int Ly,
+                                                       int* scratch, int ltid, int nw, Sync sync) {
+  const int lane = ltid & 31, wid = ltid >> 5;
   const int N = Lx * Ly;
   int* kx = scratch;           // (2, Lx) occupied sites per row
   int* kpx = scratch + 2 * Lx;  // (2, Lx) occupied sites with y >= 1 per row
@@ -65,9 +68,9 @@ __device__ __forceinline__ int image_sign_parity(const int* simg, int g, int Lx,
       kpx[r] = __popc(b & ~1u);
     }
   }
-  __syncthreads();
+  sync();
   int par = 0;
-  if (threadIdx.x == 0 && g != 0) {
+  if (ltid == 0 && g != 0) {
     int nsec[2] = {0, 0};
     for (int sg = 0; sg < 2; ++sg) {
       long long S = 0, Q = 0, Y = 0;
@@ -85,7 +88,17 @@ __device__ __forceinline__ int image_sign_parity(const int* simg, int g, int Lx,
     }
     if (g & 4) par ^= (nsec[0] * nsec[1]) & 1;
   }
-  return par;  // meaningful in thread 0
+  return par;  // meaningful in thread 0 of the group
+}
+
+struct BlockSync {
+  __device__ void operator()() const { __syncthreads(); }
+};
+
+__device__ __forceinline__ int image_sign_parity(const int* simg, int g, int Lx, int Ly,
+                                                 int* scratch) {
+  return image_sign_parity_group(simg, g, Lx, Ly, scratch, (int)threadIdx.x,
+                                 (int)(blockDim.x >> 5), BlockSync{});
 }
 
 // ------------------------------------------------------------------ Philox4x32-10
