@@ -24,6 +24,9 @@
 // Output: the occupied rows Y (n, d) FP32 of the image configuration, the occupied-mode list and
 // the item sign, like the CUDA-core kernel (mode 1 of nh_cnn.cu).
 //
+// The packed weight image (129 KB) is brought into shared memory once per CTA by one bulk TMA
+// copy (cp.async.bulk, no multicast) that completes on an mbarrier.
+//
 // Supported: Lx = 16, Ly = 16, 32 channels, 4 layers (the benchmark network).  Every wait on an
 // mbarrier is bounded; on expiry the kernel records an error code in *err and returns after
 // releasing its tensor memory.
@@ -232,7 +235,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
   float* bsm = reinterpret_cast<float*>(act_all + kWG * kActBytes);  // (4, 32) biases
   int* ints_all = reinterpret_cast<int*>(bsm + 4 * kC);  // per group: kIntsPerWG
   uint64_t* bars = reinterpret_cast<uint64_t*>(ints_all + kWG * kIntsPerWG);  // per group
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kWG);
+  uint64_t* wbar = bars + kWG;  // completion of the weight-image bulk copy
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(wbar + 1);
   int* abort_all = reinterpret_cast<int*>(tmem_slot + 1);  // per group
 
   const int tid = threadIdx.x;
@@ -240,17 +244,27 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
   const int lane = ltid & 31, lwid = ltid >> 5;  // lwid = warp % 4: the TMEM lane quarter
   const int N = kL * kL, M2 = 2 * N;
 
-  // Weights and biases resident for the whole launch.
-  for (int i = tid; i < kWBytes / 16; i += kTcThreads)
-    reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.wpk) + i);
-  for (int i = tid; i < 4 * kC; i += kTcThreads) bsm[i] = __ldg(a.bias + i);
+  // Weights resident for the whole launch: one bulk TMA copy of the packed image (16-byte
+  // aligned, a multiple of 16 bytes; this CTA's own shared memory, no multicast), completing on
+  // wbar; the biases by plain loads.
   if (tid == 0) {
-    for (int w = 0; w < kWG; ++w) {
+    for (int w = 0; w <= kWG; ++w) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars + w)) : "memory");
-      abort_all[w] = 0;
+      if (w < kWG) abort_all[w] = 0;
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(smem_u32(wbar)),
+        "r"((uint32_t)kWBytes)
+        : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(wsm)),
+        "l"(a.wpk), "r"((uint32_t)kWBytes), "r"(smem_u32(wbar))
+        : "memory");
   }
+  for (int i = tid; i < 4 * kC; i += kTcThreads) bsm[i] = __ldg(a.bias + i);
   if (tid < 32) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
@@ -261,6 +275,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!mbar_wait(wbar, 0)) {  // the weight copy did not complete: no item is computed
+    if (tid == 0) {
+      atomicExch(a.err, 1);
+      for (int w = 0; w < kWG; ++w) abort_all[w] = 1;
+    }
+  }
+  __syncthreads();
 
   // This warp group's state.
   const uint32_t tmem = *tmem_slot + 64u * wg;
@@ -490,6 +511,8 @@ int launch_cnn_tc(const ConfigList& cl, const nh_backflow_params& p, int mode, f
     return fail(NH_ERR_UNSUPPORTED, "tensor-core CNN: %dx%d lattice, %d channels, %d layers "
                 "(supported: 16x16, 32, 4)", p.Lx, p.Ly, p.channels, p.layers);
   if (!p.conv_w_tc) return fail(NH_ERR_INVALID, "tensor-core CNN: conv_w_tc is null");
+  if (reinterpret_cast<uintptr_t>(p.conv_w_tc) % 16)
+    return fail(NH_ERR_INVALID, "tensor-core CNN: conv_w_tc must be 16-byte aligned");
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(cnn_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
