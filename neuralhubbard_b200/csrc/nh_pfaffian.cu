@@ -230,14 +230,15 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
             for (int p = 0; p < NB; ++p)
               if (p < j) c += myU[p] * Vs[ck * NB + p] - myV[p] * Us[ck * NB + p];
           }
-          // Warp max of |c| (rounded up to FP32, NaN as +inf), ties to the lowest row.
-          const float mag = act ? (isnan(c) ? INFINITY : to_key_float(fabs(c))) : -1.0f;
-          float wmax = mag;
-#pragma unroll
-          for (int o = 16; o; o >>= 1) wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
-          const unsigned hit = __ballot_sync(0xffffffffu, mag == wmax);
+          // Warp max of |c| (rounded up to FP32, NaN as +inf), ties to the lowest row, as one
+          // integer reduction: non-negative floats order like their bit patterns, and the key
+          // bits + 1 leaves 0 for rows that are no longer active.
+          const float mag = isnan(c) ? INFINITY : to_key_float(fabs(c));
+          const unsigned key = act ? __float_as_uint(mag) + 1u : 0u;
+          const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+          const unsigned hit = __ballot_sync(0xffffffffu, key == kmax);
           if (lane == __ffs(hit) - 1) {
-            rkey[wid] = wmax;
+            rkey[wid] = kmax ? __uint_as_float(kmax - 1u) : -1.0f;
             rt[wid] = tid;
             if constexpr (sizeof(T) == 4)  // FP32: |c| is the key, the sign rides in bit 31
               rlog[wid] = my_log | (signbit(c) ? (int)0x80000000 : 0);
