@@ -226,9 +226,17 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
           const bool act = my_log > k;
           if (act) {
             c = aval(Lw, tid, ck);
+            if (j > 0) {  // row ck's panel values: 16-byte loads (rows are NB * sizeof(T) apart)
+              T vr[NB], ur[NB];
 #pragma unroll
-            for (int p = 0; p < NB; ++p)
-              if (p < j) c += myU[p] * Vs[ck * NB + p] - myV[p] * Us[ck * NB + p];
+              for (int q = 0; q < NB; q += Vec<T>::k) {
+                lds16(Vs + ck * NB + q, vr + q);
+                lds16(Us + ck * NB + q, ur + q);
+              }
+#pragma unroll
+              for (int p = 0; p < NB; ++p)
+                if (p < j) c += myU[p] * vr[p] - myV[p] * ur[p];
+            }
           }
           // Warp max of |c| (rounded up to FP32, NaN as +inf), ties to the lowest row, as one
           // integer reduction: non-negative floats order like their bit patterns, and the key
@@ -284,9 +292,17 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
             T u = T(0), v = T(0);
             if (live) {
               T dv = aval(Lw, tid, r);
+              if (j > 0) {
+                T vr[NB], ur[NB];
 #pragma unroll
-              for (int p = 0; p < NB; ++p)
-                if (p < j) dv += myU[p] * Vs[r * NB + p] - myV[p] * Us[r * NB + p];
+                for (int q = 0; q < NB; q += Vec<T>::k) {
+                  lds16(Vs + r * NB + q, vr + q);
+                  lds16(Us + r * NB + q, ur + q);
+                }
+#pragma unroll
+                for (int p = 0; p < NB; ++p)
+                  if (p < j) dv += myU[p] * vr[p] - myV[p] * ur[p];
+              }
               u = dv;
               v = c * (T(1) / piv);
             }
