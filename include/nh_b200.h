@@ -4,7 +4,8 @@
  * int status (NH_OK = 0, negative on error; nh_last_error() gives the message of the calling
  * thread) and never synchronises the host unless its comment says so.  The caller owns every
  * buffer.  Entry points that need scratch memory take (workspace, workspace_bytes) and have a
- * *_workspace_bytes() query.  Configurations are int8 +-1 arrays of length 2N (spin-up sites
+ * *_workspace_bytes() query; a workspace must be 256-byte aligned, as cudaMalloc returns it
+ * (NH_ERR_INVALID otherwise).  Configurations are int8 +-1 arrays of length 2N (spin-up sites
  * first, site index x * Ly + y), as in the reference's quantax convention.
  *
  * Reference interfaces replaced (paths inside the ChenAo-Phys/NeuralHubbard tree):
@@ -30,7 +31,7 @@
 extern "C" {
 #endif
 
-#define NH_ABI_VERSION 3
+#define NH_ABI_VERSION 4
 
 enum {
   NH_OK = 0,
@@ -159,11 +160,13 @@ int nh_cnn_forward(const int8_t* spins, int batch, const nh_backflow_params* p, 
 int nh_pairing_occ(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
                    int n, int batch, float* F, void* stream);
 
-/* sign and log|pf| of batch antisymmetric n x n FP32 matrices (n even, n <= 256); only the
+/* sign and log|pf| of batch antisymmetric n x n FP32 matrices (n even, n <= 1024); only the
  * strict lower triangle is read.  With cond_tau > 0 the matrices whose pivot ratio exceeds it
- * are flagged NH_FLAG_GROWTH and factorised again in FP64 (NH_FLAG_REFINED) when n <= 232 (the FP64
- * triangle must fit in shared memory); the workspace holds the list of those matrices. */
-size_t nh_slogpf_workspace_bytes(int batch);
+ * are flagged NH_FLAG_GROWTH and factorised again in FP64 (NH_FLAG_REFINED).  The workspace
+ * (nh_slogpf_workspace_bytes(n, batch) bytes) holds the list of those matrices and, where a
+ * triangle exceeds shared memory (FP32 n > 256, FP64 n > 236), one triangle per SM; it may be
+ * null when cond_tau <= 0 and n <= 256. */
+size_t nh_slogpf_workspace_bytes(int n, int batch);
 int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, double* logabs,
               int32_t* flags, void* workspace, size_t workspace_bytes, void* stream);
 
@@ -174,14 +177,16 @@ int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, do
  * NH_SLOGPF_NOALLOC_MAX_BATCH + 64 int32 words held by every GPU that loads the library; batch
  * beyond that limit returns NH_ERR_UNSUPPORTED.  The first call on a device looks up the array's
  * address (make it before any stream capture); all calls share the array, so calls that overlap
- * on the GPU race.  Allocates nothing.  Same results as nh_slogpf. */
+ * on the GPU race.  Allocates nothing.  n <= 256; same results as nh_slogpf for n <= 236, while
+ * for 236 < n <= 256 flagged matrices keep their FP32 result (the FP64 triangle would need
+ * workspace). */
 #define NH_SLOGPF_NOALLOC_MAX_BATCH 65536
 int nh_slogpf_noalloc(const float* F, int n, int batch, double cond_tau, float* sign,
                       double* logabs, int32_t* flags, void* stream);
 
 /* Amplitudes of batch configurations.  n_symm = 1: psi(s); n_symm = 8: the projection onto the
  * trivial representation of Flip(0) Flip(1) SpinInverse, psi_P(s) = 1/8 sum_g eta_g psi(g s).
- * Lattices up to 32 x 32 and n = n_up + n_dn <= 1024: beyond n = 256 (FP32) / 232 (FP64) the
+ * Lattices up to 32 x 32 and n = n_up + n_dn <= 1024: beyond n = 256 (FP32) / 236 (FP64) the
  * Pfaffian keeps its triangles, and beyond shared memory the CNN its activation planes, in a
  * per-CTA scratch that the workspace query includes (e.g. ~0.4 GB at 32 x 32). */
 size_t nh_amplitude_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p);

@@ -73,7 +73,7 @@ SIGNATURES = {
     "nh_cnn_forward": (c_int, [c_void_p, c_int, P_BF, c_void_p, c_void_p]),
     "nh_pairing_occ": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int,
                                c_void_p, c_void_p]),
-    "nh_slogpf_workspace_bytes": (c_size_t, [c_int]),
+    "nh_slogpf_workspace_bytes": (c_size_t, [c_int, c_int]),
     "nh_slogpf": (c_int, [c_void_p, c_int, c_int, c_double, c_void_p, c_void_p, c_void_p,
                           c_void_p, c_size_t, c_void_p]),
     "nh_slogpf_noalloc": (c_int, [c_void_p, c_int, c_int, c_double, c_void_p, c_void_p, c_void_p,

@@ -125,9 +125,9 @@ DEFAULT_CANCEL_TAU = 8.0
 
 def slogpf(F: torch.Tensor, cond_tau: float = DEFAULT_COND_TAU):
     """(sign FP32, logabs FP64, flags int32) of the Pfaffians of antisymmetric F (..., n, n)
-    in FP32; only the strict lower triangle is read.  Matrices whose pivot ratio exceeds
-    ``cond_tau`` are factorised again in FP64 (flags NH_FLAG_GROWTH | NH_FLAG_REFINED);
-    ``cond_tau=0`` keeps the plain FP32 result."""
+    in FP32, n even and at most 1024; only the strict lower triangle is read.  Matrices whose
+    pivot ratio exceeds ``cond_tau`` are factorised again in FP64 (flags NH_FLAG_GROWTH |
+    NH_FLAG_REFINED); ``cond_tau=0`` keeps the plain FP32 result."""
     F = _require_cuda(F, torch.float32, "F")
     n = F.shape[-1]
     if F.shape[-2] != n:
@@ -137,7 +137,7 @@ def slogpf(F: torch.Tensor, cond_tau: float = DEFAULT_COND_TAU):
     sign = torch.empty(batch, dtype=torch.float32, device=F.device)
     logabs = torch.empty(batch, dtype=torch.float64, device=F.device)
     flags = torch.empty(batch, dtype=torch.int32, device=F.device)
-    nbytes = _lib.load().nh_slogpf_workspace_bytes(batch)
+    nbytes = _lib.load().nh_slogpf_workspace_bytes(n, batch)
     ws = workspace(nbytes, F.device, "slogpf")
     _lib.call("nh_slogpf", F.data_ptr(), n, batch, float(cond_tau), sign.data_ptr(),
               logabs.data_ptr(), flags.data_ptr(), ws.data_ptr(), ws.numel(),

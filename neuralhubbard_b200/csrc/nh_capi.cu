@@ -76,6 +76,14 @@ int check_cuda(cudaError_t e, const char* what) {
 
 int check_launch(const char* what) { return check_cuda(cudaGetLastError(), what); }
 
+int check_workspace(const void* ws, size_t have, size_t need, const char* who) {
+  if (!ws || have < need)
+    return fail(NH_ERR_WORKSPACE, "%s: workspace %zu < %zu bytes", who, ws ? have : 0, need);
+  if (reinterpret_cast<uintptr_t>(ws) % 256)
+    return fail(NH_ERR_INVALID, "%s: workspace %p is not 256-byte aligned", who, ws);
+  return NH_OK;
+}
+
 int num_sms() {
   int dev = 0, n = 0;
   cudaGetDevice(&dev);
@@ -281,28 +289,40 @@ int nh_pairing_occ(const float* Y, const int32_t* idx, const float* Wt, int Lx, 
   return launch_pairing(Y, idx, Wt, Lx, Ly, d, n, batch, F, static_cast<cudaStream_t>(stream));
 }
 
-size_t nh_slogpf_workspace_bytes(int batch) {
-  return align256((size_t)(batch > 0 ? batch : 1) * sizeof(int32_t)) + align256(sizeof(int32_t));
+// Layout: [per-CTA triangles when n exceeds shared memory][refinement list (batch)][count].
+size_t nh_slogpf_workspace_bytes(int n, int batch) {
+  const size_t tri = (n > 0 && n % 2 == 0 && n <= kMaxN) ? align256(pfaffian_scratch_bytes(n)) : 0;
+  return tri + align256((size_t)(batch > 0 ? batch : 1) * sizeof(int32_t)) +
+         align256(sizeof(int32_t));
 }
 
 int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, double* logabs,
               int32_t* flags, void* workspace, size_t workspace_bytes, void* stream) {
   if (!F || !sign || !logabs || batch < 0) return fail(NH_ERR_INVALID, "slogpf: bad arguments");
+  if (n <= 0 || n % 2 || n > kMaxN)
+    return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d must be even and <= %d", n, kMaxN);
+  const bool refine = cond_tau > 0.0;
+  if (refine && !flags) return fail(NH_ERR_INVALID, "slogpf: refinement needs flags");
   if (batch == 0) return NH_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const bool refine = cond_tau > 0.0;
-  if (refine && (!flags || !workspace || workspace_bytes < nh_slogpf_workspace_bytes(batch)))
-    return fail(NH_ERR_WORKSPACE, "slogpf: refinement needs flags and %zu B of workspace",
-                nh_slogpf_workspace_bytes(batch));
-  int rc = launch_pfaffian_from_F(F, n, batch, nullptr, nullptr, false, cond_tau, 0, sign,
-                                  logabs, flags, st);
-  if (rc || !refine || !pfaffian64_fits(n)) return rc;  // too large for FP64: flags only
-  int32_t* list = static_cast<int32_t*>(workspace);
-  int32_t* count = reinterpret_cast<int32_t*>(static_cast<char*>(workspace) +
-                                              align256((size_t)batch * sizeof(int32_t)));
+  // Scratch: the FP64 triangles when refining, the FP32 ones beyond n = 256.
+  const bool scratch = pfaffian_needs_scratch(n, refine);
+  int rc;
+  if ((refine || scratch) &&
+      (rc = check_workspace(workspace, workspace_bytes, nh_slogpf_workspace_bytes(n, batch),
+                            "slogpf")))
+    return rc;
+  const size_t tri_bytes = align256(pfaffian_scratch_bytes(n));
+  void* tri = tri_bytes ? workspace : nullptr;
+  rc = launch_pfaffian_from_F(F, n, batch, nullptr, nullptr, false, cond_tau, 0, sign, logabs,
+                              flags, tri, st);
+  if (rc || !refine) return rc;
+  char* w = static_cast<char*>(workspace) + tri_bytes;
+  int32_t* list = reinterpret_cast<int32_t*>(w);
+  int32_t* count = reinterpret_cast<int32_t*>(w + align256((size_t)batch * sizeof(int32_t)));
   if ((rc = launch_flagged(flags, batch, nullptr, 1, list, count, st))) return rc;
   return launch_pfaffian_from_F(F, n, batch, list, count, true, 0.0,
-                                NH_FLAG_GROWTH | NH_FLAG_REFINED, sign, logabs, flags, st);
+                                NH_FLAG_GROWTH | NH_FLAG_REFINED, sign, logabs, flags, tri, st);
 }
 
 size_t nh_amplitude_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p) {
@@ -320,8 +340,7 @@ int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_p
   if (n_symm != 1 && n_symm != 8) return fail(NH_ERR_INVALID, "amplitude: n_symm %d (1 or 8)", n_symm);
   if (batch == 0) return NH_OK;
   const size_t need = nh_amplitude_workspace_bytes(batch, n_symm, p);
-  if (!workspace || workspace_bytes < need)
-    return fail(NH_ERR_WORKSPACE, "amplitude: workspace %zu < %zu bytes", workspace_bytes, need);
+  if ((rc = check_workspace(workspace, workspace_bytes, need, "amplitude"))) return rc;
   const int n = p->n_up + p->n_dn, d = p->channels / 2;
   PipelineBuffers b = carve_pipeline(workspace, batch * n_symm, n, d, p->Lx * p->Ly, p->channels);
   ConfigList cl{spins, nullptr, nullptr, nullptr, nullptr, batch, n_symm};
@@ -394,8 +413,7 @@ int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs
   if (batch == 0) return NH_OK;
   const int chunk = chunk_configs > 0 ? chunk_configs : kDefaultChunk;
   const size_t need = nh_local_energy_workspace_bytes(batch, n_symm, chunk, p);
-  if (!workspace || workspace_bytes < need)
-    return fail(NH_ERR_WORKSPACE, "local_energy: workspace %zu < %zu bytes", workspace_bytes, need);
+  if ((rc = check_workspace(workspace, workspace_bytes, need, "local_energy"))) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   ElocLayout L = eloc_layout(workspace, batch, n_symm, chunk, p, 8);
   const int N = p->Lx * p->Ly, n = p->n_up + p->n_dn, d = p->channels / 2;
@@ -504,8 +522,7 @@ int nh_metropolis_steps(int8_t* spins, float* sign, double* logabs, int batch, i
   if (n_symm != 1 && n_symm != 8) return fail(NH_ERR_INVALID, "metropolis: n_symm %d", n_symm);
   if (batch == 0 || nsteps == 0) return NH_OK;
   const size_t need = nh_metropolis_workspace_bytes(batch, n_symm, p);
-  if (!workspace || workspace_bytes < need)
-    return fail(NH_ERR_WORKSPACE, "metropolis: workspace %zu < %zu bytes", workspace_bytes, need);
+  if ((rc = check_workspace(workspace, workspace_bytes, need, "metropolis"))) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   MhLayout L = mh_layout(workspace, batch, n_symm, p);
   const int n = p->n_up + p->n_dn, d = p->channels / 2, N = p->Lx * p->Ly;
@@ -549,9 +566,7 @@ int nh_metropolis_steps_learned(int8_t* spins, float* sign, double* logabs, int 
     return fail(NH_ERR_INVALID, "metropolis_learned: n_symm %d", n_symm);
   if (batch == 0 || nsteps == 0) return NH_OK;
   const size_t need = nh_metropolis_learned_workspace_bytes(batch, n_symm, p);
-  if (!workspace || workspace_bytes < need)
-    return fail(NH_ERR_WORKSPACE, "metropolis_learned: workspace %zu < %zu bytes",
-                workspace_bytes, need);
+  if ((rc = check_workspace(workspace, workspace_bytes, need, "metropolis_learned"))) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   MhLayout L = mh_layout(workspace, batch, n_symm, p);
   const int n = p->n_up + p->n_dn, d = p->channels / 2, N = p->Lx * p->Ly;

@@ -260,8 +260,6 @@ constexpr int kCnnBigPerSm = 4;  // CTAs per SM of the global-activation kernel 
 
 }  // namespace
 
-bool cnn64_fits(int N, int C) { return cnn_smem<double>(N, C) <= 227 * 1024; }
-
 int launch_pack_cnn(const float* conv_w, int channels, int layers, float* packed, cudaStream_t st) {
   const int total = 18 * channels + (layers - 1) * 9 * channels * channels;
   ProfScope prof_scope(NH_K_PACK, st);

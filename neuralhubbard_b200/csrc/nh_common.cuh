@@ -16,6 +16,9 @@ void set_error(const char* fmt, ...);
 int fail(int code, const char* fmt, ...);
 int check_cuda(cudaError_t e, const char* what);
 int check_launch(const char* what);
+// Caller workspaces: NH_ERR_WORKSPACE when null or smaller than need, NH_ERR_INVALID when not
+// 256-byte aligned (every carve offset is a multiple of 256 and the kernels use 16-byte vectors).
+int check_workspace(const void* ws, size_t have, size_t need, const char* who);
 
 // ------------------------------------------------------------------ lattice helpers
 // Mode m = sigma * N + x * Ly + y.  Symmetry element g = fx + 2 fy + 4 si:
@@ -196,9 +199,12 @@ struct PfGatherArgs {
 // Launchers (return NH_OK or an error code).
 int launch_cnn(const CnnLaunch& q, cudaStream_t st);
 int launch_pack_cnn(const float* conv_w, int channels, int layers, float* packed, cudaStream_t st);
+// tri: pfaffian_scratch_bytes(n) of per-CTA triangles, required when pfaffian_needs_scratch(n,
+// fp64) (n up to 1024), else unused and may be null.
 int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list,
                            const int32_t* count, bool fp64, double cond_tau, int flag_or,
-                           float* sign, double* logabs, int32_t* flags, cudaStream_t st);
+                           float* sign, double* logabs, int32_t* flags, void* tri,
+                           cudaStream_t st);
 int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st);
 // Tensor-memory Pfaffian (one matrix per SM, trailing updates on tcgen05): mode 1 gathers from
 // g.Y / g.idx / g.Wt (FP32), mode 0 reads dense F (items, n, n) FP32.
@@ -224,9 +230,8 @@ bool cnn_tc_supported(const nh_backflow_params& p);
 int launch_pack_cnn_tc(const float* conv_w, uint16_t* packed, cudaStream_t st);
 int launch_cnn_tc(const ConfigList& cl, const nh_backflow_params& p, int mode, float* Y,
                   int32_t* idx, float* item_sign, int32_t* err, cudaStream_t st);
-// Whether the FP64 kernels fit in shared memory (n x n Pfaffian; N sites x C channels CNN).
+// Whether the FP64 Pfaffian of an n x n matrix fits in shared memory.
 bool pfaffian64_fits(int n);
-bool cnn64_fits(int N, int C);
 // Large lattices: bytes of global scratch the Pfaffian (FP32 and FP64) and the CNN need when
 // their working set exceeds shared memory (0 when it does not).
 bool pfaffian_needs_scratch(int n, bool fp64);

@@ -59,19 +59,23 @@ extern "C" int nh_slogpf_noalloc(const float* F, int n, int batch, double cond_t
   if (batch > kNoAllocMaxBatch)
     return fail(NH_ERR_UNSUPPORTED, "slogpf_noalloc: batch %d exceeds the static scratch limit %d",
                 batch, kNoAllocMaxBatch);
-  if (batch == 0) return NH_OK;
+  if (n <= 0 || n % 2 || n > kNumThreads)
+    return fail(NH_ERR_UNSUPPORTED,
+                "slogpf_noalloc: n=%d must be even and <= %d (beyond, nh_slogpf with a workspace)",
+                n, kNumThreads);
   const bool refine = cond_tau > 0.0;
   if (refine && !flags) return fail(NH_ERR_INVALID, "slogpf_noalloc: refinement needs flags");
+  if (batch == 0) return NH_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int32_t* scratch = nullptr;
   int rc = scratch_address(&scratch);
   if (rc) return rc;
   rc = launch_pfaffian_from_F(F, n, batch, nullptr, nullptr, false, cond_tau, 0, sign, logabs,
-                              flags, st);
+                              flags, nullptr, st);
   if (rc || !refine || !pfaffian64_fits(n)) return rc;
   int32_t* list = scratch;
   int32_t* count = scratch + kNoAllocMaxBatch;  // written by the listing kernel on every call
   if ((rc = launch_flagged(flags, batch, nullptr, 1, list, count, st))) return rc;
   return launch_pfaffian_from_F(F, n, batch, list, count, true, 0.0,
-                                NH_FLAG_GROWTH | NH_FLAG_REFINED, sign, logabs, flags, st);
+                                NH_FLAG_GROWTH | NH_FLAG_REFINED, sign, logabs, flags, nullptr, st);
 }

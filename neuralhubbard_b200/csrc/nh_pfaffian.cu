@@ -479,7 +479,7 @@ int launch_pf(const PfArgs& a, cudaStream_t st) {
 }
 
 // FP32: the widest panel that keeps two CTAs per SM; FP64: one CTA per SM; beyond shared
-// memory (FP32 n > 256, FP64 n > 232): the large-lattice kernel.
+// memory (FP32 n > 256, FP64 n > 236): the large-lattice kernel.
 template <typename T, int D>
 int launch_pf_pick(const PfArgs& a, cudaStream_t st) {
   if (a.n <= kNumThreads) {
@@ -1148,9 +1148,10 @@ size_t pfaffian_scratch_bytes(int n) {
 
 int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list,
                            const int32_t* count, bool fp64, double cond_tau, int flag_or,
-                           float* sign, double* logabs, int32_t* flags, cudaStream_t st) {
-  if (n <= 0 || n % 2 || n > kNumThreads)
-    return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d must be even and <= %d", n, kNumThreads);
+                           float* sign, double* logabs, int32_t* flags, void* tri,
+                           cudaStream_t st) {
+  if (n <= 0 || n % 2 || n > kBigThreads)
+    return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d must be even and <= %d", n, kBigThreads);
   PfArgs a{};
   a.n = n;
   a.mode = 0;
@@ -1164,6 +1165,7 @@ int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list
   a.flags = flags;
   a.cond_tau = cond_tau;
   a.flag_or = flag_or;
+  a.tri = tri;
   return fp64 ? launch_pf_pick<double, 16>(a, st) : launch_pf_pick<float, 16>(a, st);
 }
 

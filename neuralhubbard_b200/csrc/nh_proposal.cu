@@ -649,9 +649,7 @@ int nh_proposal_backward(const int8_t* spins, const int32_t* moves, const float*
   if (!spins || !moves || !weights || !grad || batch <= 0)
     return fail(NH_ERR_INVALID, "proposal_backward: buffers");
   const size_t need = nh_proposal_backward_workspace_bytes(batch);
-  if (!workspace || workspace_bytes < need)
-    return fail(NH_ERR_WORKSPACE, "proposal_backward: workspace %zu < %zu bytes",
-                workspace_bytes, need);
+  if ((rc = check_workspace(workspace, workspace_bytes, need, "proposal_backward"))) return rc;
   const size_t smem = prop_backward_smem(q->Lx * q->Ly);
   if (smem > kSmemLimit)
     return fail(NH_ERR_UNSUPPORTED, "proposal_backward: %d sites exceed shared memory",

@@ -42,12 +42,14 @@ def rand_skew32(rng, n, batch):
     return A - np.swapaxes(A, 1, 2)
 
 
-@pytest.mark.parametrize("n", [2, 4, 56, 100, 224, 256])
+@pytest.mark.parametrize("n", [2, 4, 56, 100, 224, 236, 248, 256, 400, 1024])
 def test_slogpf_random(n):
     """Gaussian antisymmetric matrices (condition ~ n^2): plain FP32, and with the FP64
-    recompute of the matrices whose pivot ratio exceeds 100."""
+    recompute of the matrices whose pivot ratio exceeds 100.  Beyond shared memory (FP32
+    n > 256, FP64 n > 236) the triangles live in the workspace; cond_tau = 1 recomputes every
+    matrix in FP64."""
     rng = np.random.default_rng(n)
-    A = rand_skew32(rng, n, 6)
+    A = rand_skew32(rng, n, 6 if n <= 400 else 3)
     s0, l0 = opf.slogpf(A.astype(np.float64))
     sg, la, fl = nh.slogpf(torch.from_numpy(A).to(DEV), cond_tau=0.0)
     assert np.array_equal(sg.cpu().numpy(), s0)
@@ -57,12 +59,14 @@ def test_slogpf_random(n):
     assert np.array_equal(sg.cpu().numpy(), s0)
     err = np.abs(la.cpu().numpy() - l0)
     refined = (fl & _lib.FLAG_REFINED) != 0
-    if n <= 224:  # the FP64 triangle fits in shared memory
-        assert np.array_equal(refined, (fl & _lib.FLAG_GROWTH) != 0)
-    else:
-        assert not refined.any()
+    assert np.array_equal(refined, (fl & _lib.FLAG_GROWTH) != 0)
     assert np.all(err[refined] < 1e-9)
     assert np.max(err) < (1e-4 if n <= 100 else 1e-3)
+    if n >= 236:
+        sg, la, fl = nh.slogpf(torch.from_numpy(A).to(DEV), cond_tau=1.0)
+        assert np.all(fl.cpu().numpy() & _lib.FLAG_REFINED)
+        assert np.array_equal(sg.cpu().numpy(), s0)
+        assert np.max(np.abs(la.cpu().numpy() - l0)) < 1e-9
 
 
 def test_slogpf_near_nodal():

@@ -37,10 +37,48 @@ def test_library_exports_every_header_symbol():
     assert lib.nh_abi_version() == want
 
 
+def header_arg_counts():
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for name, args in re.findall(r"\b(nh_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", text):
+        args = " ".join(args.split())
+        out[name] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
 def test_ctypes_table_matches_header():
     from neuralhubbard_b200 import _lib
 
     assert sorted(_lib.SIGNATURES) == header_symbols()
+    counts = header_arg_counts()
+    for name, (_, argtypes) in _lib.SIGNATURES.items():
+        assert len(argtypes) == counts[name], name
+
+
+def test_argument_checks_before_device_work():
+    """Entry points refuse bad sizes, missing buffers and bad workspaces with the documented
+    status and message before touching the device (fake, never-dereferenced pointers)."""
+    if not os.path.exists(LIB):
+        pytest.skip("libnh_b200.so not built")
+    from neuralhubbard_b200 import _lib
+
+    lib = _lib.load()
+    p = ctypes.c_void_p(4096)
+
+    def slogpf(n, flags=p, ws=p, nbytes=1 << 20, tau=100.0):
+        return lib.nh_slogpf(p, n, 4, tau, p, p, flags, ws, nbytes, None)
+
+    assert slogpf(7) == -2 and b"must be even" in lib.nh_last_error()
+    assert slogpf(1026) == -2
+    assert lib.nh_slogpf(None, 56, 4, 100.0, p, p, p, p, 1 << 20, None) == -1
+    assert slogpf(56, flags=None) == -1 and b"needs flags" in lib.nh_last_error()
+    assert slogpf(56, nbytes=16) == -4
+    assert slogpf(56, ws=None) == -4
+    assert slogpf(56, ws=ctypes.c_void_p(4096 + 16)) == -1
+    assert b"256-byte aligned" in lib.nh_last_error()
+    assert lib.nh_slogpf_noalloc(p, 300, 4, 100.0, p, p, p, None) == -2
+    assert lib.nh_slogpf_workspace_bytes(56, 4) == lib.nh_slogpf_workspace_bytes(56, 64)
+    assert lib.nh_slogpf_workspace_bytes(56, 65) > lib.nh_slogpf_workspace_bytes(56, 64)
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):

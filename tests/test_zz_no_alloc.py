@@ -43,7 +43,7 @@ def _run(fn_name, F, n, B, tau, with_ws):
     flags = torch.empty(B, dtype=torch.int32, device=dev)
     st = torch.cuda.current_stream().cuda_stream
     if with_ws:
-        ws = torch.empty(lib.nh_slogpf_workspace_bytes(B), dtype=torch.uint8, device=dev)
+        ws = torch.empty(lib.nh_slogpf_workspace_bytes(n, B), dtype=torch.uint8, device=dev)
         rc = lib.nh_slogpf(F.data_ptr(), n, B, tau, sign.data_ptr(), logabs.data_ptr(),
                            flags.data_ptr(), ws.data_ptr(), ws.numel(), st)
     else:
@@ -74,3 +74,13 @@ def test_noalloc_rejects_oversized_batch():
                                ctypes.c_void_p(8), ctypes.c_void_p(8), None)
     assert rc == -2
     assert b"exceeds the static scratch limit" in lib.nh_last_error()
+
+
+def test_noalloc_rejects_large_n():
+    """Triangles beyond shared memory need workspace: n > 256 is refused with a pointer to
+    nh_slogpf."""
+    lib = _lib.load()
+    rc = lib.nh_slogpf_noalloc(ctypes.c_void_p(8), 300, 4, 100.0, ctypes.c_void_p(8),
+                               ctypes.c_void_p(8), ctypes.c_void_p(8), None)
+    assert rc == -2
+    assert b"nh_slogpf with a workspace" in lib.nh_last_error()
