@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define NH_ABI_VERSION 4
+#define NH_ABI_VERSION 5
 
 enum {
   NH_OK = 0,
@@ -50,12 +50,25 @@ enum {
   NH_FLAG_CANCEL = 16      /* projected amplitude: sum_g |psi_g| > cancel_tau |sum_g eta_g psi_g| */
 };
 
+/* Backflow networks (nh_backflow_params.net). */
+#define NH_NET_CNN 0     /* periodic 3x3 CNN on the +-1 occupation image (layers conv layers) */
+#define NH_NET_RESCONV 1 /* residual CNN of the released states (layers residual blocks) */
+
 /* Parameters of the backflow network (device pointers).
- * conv_w:        FP32, layers concatenated, layer l of shape (C_out, C_in, 3, 3) (C_in = 2 for
- *                l = 0, else channels); conv_b: FP32, (channels,) per layer, concatenated.
- *                The features are the last layer's channels: [0, d) spin up, [d, 2d) spin
+ * net:           NH_NET_CNN or NH_NET_RESCONV.
+ * conv_w:        NH_NET_CNN: FP32, layers concatenated, layer l of shape (C_out, C_in, 3, 3)
+ *                (C_in = 2 for l = 0, else channels); conv_b: FP32, (channels,) per layer.
+ *                NH_NET_RESCONV (channels 64, cnn_mode 0): the occupation embedding (C, 4)
+ *                (occupation index n_up + 2 n_dn: empty, up, down, double) followed by the
+ *                2 * layers convolutions (C, C, 3, 3) of the residual blocks
+ *                x + Conv2(GELU(Conv1(GELU(RMSNorm(x))))) in order; conv_b: (2 * layers, C).
+ *                RMSNorm is over all channels and sites without affine parameters; the
+ *                features are the last block's output divided by sqrt(layers + 1)
+ *                (code/backflow/models.py:319-329, quantax ResConv).
+ *                Either way the features are the last channels [0, d) spin up, [d, 2d) spin
  *                down, d = channels / 2.
- * conv_w_packed: the same weights repacked by nh_pack_cnn_weights (read by the kernels).
+ * conv_w_packed: the same weights repacked by nh_pack_cnn_weights (NH_NET_CNN) or
+ *                nh_pack_resconv_weights (NH_NET_RESCONV, 16-byte aligned); read by the kernels.
  * conv_w_tc:     BF16 hi/lo tensor-core layout from nh_pack_cnn_weights_tc (cnn_mode 1 and 2).
  * cnn_mode:      0 = FP32 CUDA cores; 1 = tcgen05 BF16; 2 = tcgen05 BF16 x3 (hi*hi + hi*lo +
  *                lo*hi, near-FP32).  Modes 1 and 2 need a 16x16 lattice, 32 channels, 4 layers.
@@ -89,6 +102,8 @@ typedef struct {
   int32_t layers;
   int32_t cnn_mode;
   int32_t pf_mode;
+  int32_t net;
+  int32_t reserved;
   double cond_tau;
   double cancel_tau;
 } nh_backflow_params;
@@ -131,6 +146,8 @@ enum {
   NH_K_PROP_FORWARD = 19,
   NH_K_PROP_BACKWARD = 20,
   NH_K_PROP_ADAM = 21,
+  NH_K_RESCONV = 22,
+  NH_K_RESCONV64 = 23,
   NH_K_COUNT = 24
 };
 int nh_profile_enable(int on);
@@ -145,13 +162,20 @@ int nh_build_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* W
 int nh_pack_cnn_weights(const float* conv_w, int channels, int layers, float* packed,
                         void* stream);
 
+/* Residual network: packed (nh_pack_resconv_weights_floats(channels, blocks) floats) =
+ * embedding as [occupation][co], then every convolution as [ci][tap][co]. */
+size_t nh_pack_resconv_weights_floats(int channels, int blocks);
+int nh_pack_resconv_weights(const float* conv_w, int channels, int blocks, float* packed,
+                            void* stream);
+
 /* Tensor-core weight image (nh_pack_cnn_weights_tc_bytes() bytes): BF16 hi and lo parts in the
  * K-major core-matrix layout; 32 channels, 4 layers. */
 size_t nh_pack_cnn_weights_tc_bytes(void);
 int nh_pack_cnn_weights_tc(const float* conv_w, int channels, int layers, void* packed,
                            void* stream);
 
-/* Features y (batch, 2, N, d) of batch configurations (no symmetry image). */
+/* Features y (batch, 2, N, d) of batch configurations (no symmetry image).  The residual network
+ * runs here up to N = 256 (beyond, its activation planes need nh_amplitude's workspace). */
 int nh_cnn_forward(const int8_t* spins, int batch, const nh_backflow_params* p, float* features,
                    void* stream);
 

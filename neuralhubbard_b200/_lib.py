@@ -14,6 +14,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libnh_b200.so")
 
 NH_OK = 0
+NET_CNN, NET_RESCONV = 0, 1
 FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH, FLAG_REFINED, FLAG_CANCEL = 1, 2, 4, 8, 16
 
 c_void_p, c_int, c_int64, c_uint64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64
@@ -40,6 +41,8 @@ class BackflowParams(ctypes.Structure):
         ("layers", ctypes.c_int32),
         ("cnn_mode", ctypes.c_int32),
         ("pf_mode", ctypes.c_int32),
+        ("net", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
         ("cond_tau", c_double),
         ("cancel_tau", c_double),
     ]
@@ -68,6 +71,8 @@ SIGNATURES = {
     "nh_build_wtilde": (c_int, [c_void_p, c_float, c_int, c_int, c_int, c_void_p, c_void_p,
                                 c_void_p]),
     "nh_pack_cnn_weights": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
+    "nh_pack_resconv_weights_floats": (c_size_t, [c_int, c_int]),
+    "nh_pack_resconv_weights": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "nh_pack_cnn_weights_tc_bytes": (c_size_t, []),
     "nh_pack_cnn_weights_tc": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "nh_cnn_forward": (c_int, [c_void_p, c_int, P_BF, c_void_p, c_void_p]),
@@ -141,7 +146,7 @@ KERNEL_IDS = {
     "hop_emit": 6, "eloc_reduce": 7, "mh_propose": 8, "compact": 9, "mh_accept": 10,
     "wtilde": 11, "pfaffian64": 12, "cnn64": 13, "flagged": 14, "pack": 15, "cnn_tc": 16,
     "pfaffian_tc": 17, "prop_sample": 18, "prop_forward": 19, "prop_backward": 20,
-    "prop_adam": 21,
+    "prop_adam": 21, "resconv": 22, "resconv64": 23,
 }
 K_COUNT = 24
 

@@ -147,7 +147,9 @@ def slogpf(F: torch.Tensor, cond_tau: float = DEFAULT_COND_TAU):
 
 class PfaffianBackflow:
     """psi(s) = pf[n * f(n) * n] * fermion_inverse_sign(s) (``models.py:121-211``) with the
-    backflow CNN of the graded configurations; parameters live on the GPU in FP32."""
+    backflow CNN of the graded configurations, or, for parameters with ``net="resconv"`` (a
+    released state, ``checkpoint.load_pfaffian_backflow``), the residual CNN of
+    ``models.py:319-329``; parameters live on the GPU in FP32."""
 
     def __init__(self, Lx: int, Ly: int, n_up: int, n_dn: int, params: Optional[dict] = None,
                  channels: int = 32, layers: int = 4, seed: int = 0, device="cuda",
@@ -166,23 +168,32 @@ class PfaffianBackflow:
         self.cancel_tau = float(cancel_tau)
         if params is None:
             params = init_params(Lx, Ly, channels, layers, seed=seed)
+        self.net = _lib.NET_RESCONV if params.get("net", "cnn") == "resconv" else _lib.NET_CNN
         self.channels = int(params["conv_w"][0].shape[0])
-        self.layers = len(params["conv_w"])
+        # residual network: ``layers`` counts blocks of two convolutions
+        self.layers = len(params["conv_w"]) // (2 if self.net == _lib.NET_RESCONV else 1)
         self.geom = PairGeometry(Lx, Ly, self.channels // 2, n_up, n_dn)
         self.host_params = params
         self.set_params(params)
 
     def set_params(self, params: dict) -> None:
         dev = self.device
+        head = [np.asarray(params["embed"], np.float32).ravel()] if self.net else []
         self.conv_w = torch.from_numpy(np.concatenate(
-            [np.asarray(w, np.float32).ravel() for w in params["conv_w"]])).to(dev)
+            head + [np.asarray(w, np.float32).ravel() for w in params["conv_w"]])).to(dev)
         self.conv_b = torch.from_numpy(np.concatenate(
             [np.asarray(b, np.float32).ravel() for b in params["conv_b"]])).to(dev)
-        self.conv_w_packed = torch.empty_like(self.conv_w)
-        _lib.call("nh_pack_cnn_weights", self.conv_w.data_ptr(), self.channels, self.layers,
-                  self.conv_w_packed.data_ptr(), stream_ptr(dev))
+        if self.net == _lib.NET_RESCONV:
+            nf = _lib.load().nh_pack_resconv_weights_floats(self.channels, self.layers)
+            self.conv_w_packed = torch.empty(nf, dtype=torch.float32, device=dev)
+            _lib.call("nh_pack_resconv_weights", self.conv_w.data_ptr(), self.channels,
+                      self.layers, self.conv_w_packed.data_ptr(), stream_ptr(dev))
+        else:
+            self.conv_w_packed = torch.empty_like(self.conv_w)
+            _lib.call("nh_pack_cnn_weights", self.conv_w.data_ptr(), self.channels,
+                      self.layers, self.conv_w_packed.data_ptr(), stream_ptr(dev))
         self.conv_w_tc = None
-        if self.channels == 32 and self.layers == 4:
+        if self.net == _lib.NET_CNN and self.channels == 32 and self.layers == 4:
             nbytes = _lib.load().nh_pack_cnn_weights_tc_bytes()
             self.conv_w_tc = torch.empty(nbytes, dtype=torch.uint8, device=dev)
             _lib.call("nh_pack_cnn_weights_tc", self.conv_w.data_ptr(), self.channels,
@@ -198,7 +209,7 @@ class PfaffianBackflow:
                                    self.conv_w_packed.data_ptr(), _ptr(self.conv_w_tc),
                                    self.Wt.data_ptr(), self.Wt64.data_ptr(), g.LX, g.LY, g.n_up,
                                    g.n_dn, self.channels, self.layers, self.cnn_mode, self.pf_mode,
-                                   self.cond_tau, self.cancel_tau)
+                                   self.net, 0, self.cond_tau, self.cancel_tau)
 
     def features(self, spins: torch.Tensor) -> torch.Tensor:
         """(B, 2, N, d) backflow features of int8 configurations (B, 2N)."""

@@ -93,18 +93,26 @@ int num_sms() {
 
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-size_t pipeline_bytes(int max_items, int n, int d, int N, int C) {
+// Activation-plane scratch of the backflow network (0 when its planes fit in shared memory).
+static size_t act_scratch_bytes(const nh_backflow_params& p) {
+  const int N = p.Lx * p.Ly;
+  return p.net == NH_NET_RESCONV ? resconv_scratch_bytes(N) : cnn_scratch_bytes(N, p.channels);
+}
+
+size_t pipeline_bytes(int max_items, const nh_backflow_params& p) {
   const size_t it = (size_t)(max_items > 0 ? max_items : 1);
+  const size_t n = (size_t)(p.n_up + p.n_dn), d = (size_t)(p.channels / 2);
   return align256(it * n * d * sizeof(float)) + align256(it * n * sizeof(int32_t)) +
          align256(it * sizeof(float)) * 2 + align256(it * sizeof(double)) +
          align256(it * sizeof(int32_t)) * 2 + align256(sizeof(int32_t)) +
          align256(it * n * d * sizeof(double)) + align256(it * n * sizeof(int32_t)) +
-         align256(sizeof(int32_t)) + align256(pfaffian_scratch_bytes(n)) +
-         align256(cnn_scratch_bytes(N, C));
+         align256(sizeof(int32_t)) + align256(pfaffian_scratch_bytes((int)n)) +
+         align256(act_scratch_bytes(p));
 }
 
-PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d, int N, int C) {
+PipelineBuffers carve_pipeline(void* ws, int max_items, const nh_backflow_params& prm) {
   const size_t it = (size_t)(max_items > 0 ? max_items : 1);
+  const size_t n = (size_t)(prm.n_up + prm.n_dn), d = (size_t)(prm.channels / 2);
   char* p = static_cast<char*>(ws);
   auto take = [&](size_t bytes) {
     char* r = p;
@@ -123,7 +131,7 @@ PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d, int N, int
   b.Y64 = reinterpret_cast<double*>(take(it * n * d * sizeof(double)));
   b.idx64 = reinterpret_cast<int32_t*>(take(it * n * sizeof(int32_t)));
   b.err = reinterpret_cast<int32_t*>(take(sizeof(int32_t)));
-  const size_t tri_bytes = pfaffian_scratch_bytes(n), act_bytes = cnn_scratch_bytes(N, C);
+  const size_t tri_bytes = pfaffian_scratch_bytes((int)n), act_bytes = act_scratch_bytes(prm);
   b.pf_tri = tri_bytes ? take(tri_bytes) : nullptr;
   b.cnn_act = act_bytes ? take(act_bytes) : nullptr;
   return b;
@@ -185,6 +193,10 @@ static int check_params(const nh_backflow_params* p) {
   if (p->channels % 2 || (d != 8 && d != 16 && d != 32))
     return fail(NH_ERR_UNSUPPORTED, "channels %d (16, 32 or 64)", p->channels);
   if (p->layers < 1 || p->layers > 16) return fail(NH_ERR_UNSUPPORTED, "layers %d", p->layers);
+  if (p->net != NH_NET_CNN && p->net != NH_NET_RESCONV)
+    return fail(NH_ERR_INVALID, "net %d (NH_NET_CNN or NH_NET_RESCONV)", p->net);
+  if (p->net == NH_NET_RESCONV && (p->channels != 64 || p->cnn_mode != 0))
+    return fail(NH_ERR_UNSUPPORTED, "the residual network needs 64 channels and cnn_mode 0");
   if (p->cnn_mode < 0 || p->cnn_mode > 2) return fail(NH_ERR_INVALID, "cnn_mode %d", p->cnn_mode);
   if (p->cnn_mode && !cnn_tc_supported(*p))
     return fail(NH_ERR_UNSUPPORTED, "cnn_mode %d needs a 16x16 lattice, 32 channels, 4 layers",
@@ -253,6 +265,19 @@ int nh_pack_cnn_weights(const float* conv_w, int channels, int layers, float* pa
   if (!conv_w || !packed || channels < 1 || layers < 1)
     return fail(NH_ERR_INVALID, "pack_cnn_weights: bad arguments");
   return launch_pack_cnn(conv_w, channels, layers, packed, static_cast<cudaStream_t>(stream));
+}
+
+size_t nh_pack_resconv_weights_floats(int channels, int blocks) {
+  return channels > 0 && blocks > 0 ? resconv_packed_floats(channels, blocks) : 0;
+}
+
+int nh_pack_resconv_weights(const float* conv_w, int channels, int blocks, float* packed,
+                            void* stream) {
+  if (!conv_w || !packed || blocks < 1) return fail(NH_ERR_INVALID, "pack_resconv_weights: "
+                                                     "bad arguments");
+  if (channels != 64)
+    return fail(NH_ERR_UNSUPPORTED, "pack_resconv_weights: %d channels (64)", channels);
+  return launch_pack_resconv(conv_w, channels, blocks, packed, static_cast<cudaStream_t>(stream));
 }
 
 size_t nh_pack_cnn_weights_tc_bytes(void) { return cnn_tc_packed_bytes(); }
@@ -327,8 +352,7 @@ int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, do
 
 size_t nh_amplitude_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p) {
   if (!p) return 0;
-  return pipeline_bytes(batch * n_symm, p->n_up + p->n_dn, p->channels / 2, p->Lx * p->Ly,
-                        p->channels);
+  return pipeline_bytes(batch * n_symm, *p);
 }
 
 int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_params* p,
@@ -341,8 +365,7 @@ int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_p
   if (batch == 0) return NH_OK;
   const size_t need = nh_amplitude_workspace_bytes(batch, n_symm, p);
   if ((rc = check_workspace(workspace, workspace_bytes, need, "amplitude"))) return rc;
-  const int n = p->n_up + p->n_dn, d = p->channels / 2;
-  PipelineBuffers b = carve_pipeline(workspace, batch * n_symm, n, d, p->Lx * p->Ly, p->channels);
+  PipelineBuffers b = carve_pipeline(workspace, batch * n_symm, *p);
   ConfigList cl{spins, nullptr, nullptr, nullptr, nullptr, batch, n_symm};
   return run_pipeline(cl, *p, b, sign, logabs, flags, static_cast<cudaStream_t>(stream));
 }
@@ -368,7 +391,7 @@ struct ElocLayout {
 
 static ElocLayout eloc_layout(void* ws, int batch, int n_symm, int chunk,
                               const nh_backflow_params* p, int n_dirs) {
-  const int n = p->n_up + p->n_dn, d = p->channels / 2;
+  const int n = p->n_up + p->n_dn;
   const size_t cmax = (size_t)batch * n * n_dirs;
   char* q = static_cast<char*>(ws);
   ElocLayout L;
@@ -388,7 +411,7 @@ static ElocLayout eloc_layout(void* ws, int batch, int n_symm, int chunk,
   L.clogabs = reinterpret_cast<double*>(take(cmax * 8));
   L.n_chunks = (int)((cmax + chunk - 1) / chunk);
   L.chunk_cnt = reinterpret_cast<int32_t*>(take((size_t)L.n_chunks * 4));
-  L.pipe = take(pipeline_bytes(chunk * n_symm, n, d, p->Lx * p->Ly, p->channels));
+  L.pipe = take(pipeline_bytes(chunk * n_symm, *p));
   L.bytes = off;
   return L;
 }
@@ -416,7 +439,7 @@ int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs
   if ((rc = check_workspace(workspace, workspace_bytes, need, "local_energy"))) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   ElocLayout L = eloc_layout(workspace, batch, n_symm, chunk, p, 8);
-  const int N = p->Lx * p->Ly, n = p->n_up + p->n_dn, d = p->channels / 2;
+  const int N = p->Lx * p->Ly, n = p->n_up + p->n_dn;
   if ((rc = launch_hop_count(spins, batch, p->Lx, p->Ly, h->n_dirs, L.counts, st))) return rc;
   if ((rc = launch_scan_counts(L.counts, batch, L.offsets, st))) return rc;
   // At most n_dirs hops per electron: the emitted list never exceeds cmax (the emit kernel
@@ -442,7 +465,7 @@ int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs
     *n_conn_out = total;
     used = (int)((total + chunk - 1) / chunk);
   }
-  PipelineBuffers b = carve_pipeline(L.pipe, chunk * n_symm, n, d, N, p->channels);
+  PipelineBuffers b = carve_pipeline(L.pipe, chunk * n_symm, *p);
   for (int i = 0; i < used; ++i) {
     const int64_t c0 = (int64_t)i * chunk;
     ConfigList cl{spins, L.owner + c0, L.from + c0, L.to + c0, L.chunk_cnt + i, chunk, n_symm};
@@ -481,7 +504,6 @@ struct MhLayout {
 };
 
 static MhLayout mh_layout(void* ws, int batch, int n_symm, const nh_backflow_params* p) {
-  const int n = p->n_up + p->n_dn, d = p->channels / 2;
   char* q = static_cast<char*>(ws);
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -500,7 +522,7 @@ static MhLayout mh_layout(void* ws, int batch, int n_symm, const nh_backflow_par
   L.psign = reinterpret_cast<float*>(take((size_t)batch * 4));
   L.plogabs = reinterpret_cast<double*>(take((size_t)batch * 8));
   L.lqr = reinterpret_cast<float*>(take((size_t)batch * 4));
-  L.pipe = take(pipeline_bytes(batch * n_symm, n, d, p->Lx * p->Ly, p->channels));
+  L.pipe = take(pipeline_bytes(batch * n_symm, *p));
   L.bytes = off;
   return L;
 }
@@ -525,8 +547,8 @@ int nh_metropolis_steps(int8_t* spins, float* sign, double* logabs, int batch, i
   if ((rc = check_workspace(workspace, workspace_bytes, need, "metropolis"))) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   MhLayout L = mh_layout(workspace, batch, n_symm, p);
-  const int n = p->n_up + p->n_dn, d = p->channels / 2, N = p->Lx * p->Ly;
-  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, n, d, N, p->channels);
+  const int N = p->Lx * p->Ly;
+  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, *p);
   for (int t = 0; t < nsteps; ++t) {
     const int64_t step = step0 + t;
     if ((rc = launch_mh_propose(spins, batch, p->Lx, p->Ly, n_dirs, seed, step, L.valid, L.from,
@@ -569,8 +591,8 @@ int nh_metropolis_steps_learned(int8_t* spins, float* sign, double* logabs, int 
   if ((rc = check_workspace(workspace, workspace_bytes, need, "metropolis_learned"))) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   MhLayout L = mh_layout(workspace, batch, n_symm, p);
-  const int n = p->n_up + p->n_dn, d = p->channels / 2, N = p->Lx * p->Ly;
-  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, n, d, N, p->channels);
+  const int N = p->Lx * p->Ly;
+  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, *p);
   for (int t = 0; t < nsteps; ++t) {
     const int64_t step = step0 + t;
     if ((rc = launch_prop_sample(spins, batch, *q, seed, step, L.valid, L.from, L.to, L.lqr, st)))

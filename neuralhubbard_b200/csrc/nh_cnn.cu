@@ -61,33 +61,6 @@ __device__ __forceinline__ void lds8(const double* p, double* o) {
   }
 }
 
-// Exclusive block scan of one int per thread; returns the exclusive prefix, *total the sum.
-__device__ __forceinline__ int block_scan(int v, int* warp_buf, int* total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) warp_buf[wid] = x;
-  __syncthreads();
-  if (wid == 0) {
-    int w = lane < (kNumThreads / 32) ? warp_buf[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
-    }
-    if (lane < (kNumThreads / 32)) warp_buf[lane] = w;
-  }
-  __syncthreads();
-  int base = wid ? warp_buf[wid - 1] : 0;
-  *total = warp_buf[kNumThreads / 32 - 1];
-  __syncthreads();
-  return base + x - v;
-}
-
 // GACT: the two activation planes live in a per-CTA slice of global memory (large lattices,
 // where they exceed shared memory); shared memory then holds the weights and scratch only.
 template <typename T, bool GACT = false>
@@ -201,35 +174,10 @@ __global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
       }
       continue;
     }
-    // Occupied list of the image configuration, ascending (block scan over mode chunks).
-    const int per = (M2 + kNumThreads - 1) / kNumThreads;
-    const int m0 = tid * per;
-    int cnt = 0;
-    for (int m = m0; m < m0 + per && m < M2; ++m) cnt += simg[m] > 0;
-    int total;
-    int pos = block_scan(cnt, wbuf, &total);
-    for (int m = m0; m < m0 + per && m < M2; ++m)
-      if (simg[m] > 0) occl[pos++] = m;
-    __syncthreads();
-    const int n = a.n;
-    T* Ydst = a.Y + (int64_t)slot * n * d;
-    for (int o = tid; o < n * d; o += kNumThreads) {
-      const int p = o / d, aa = o - p * d;
-      const int m = occl[p < total ? p : 0];
-      const int sg = m >= N ? 1 : 0;
-      Ydst[o] = in[(sg * d + aa) * NS + (m - sg * N)];
-    }
-    int32_t* idst = a.idx + (int64_t)slot * n;
-    for (int p = tid; p < n; p += kNumThreads) idst[p] = occl[p < total ? p : 0];
-    // eta_g from per-row occupation counts (closed form of the inversion parity).
-    const int odd = image_sign_parity(simg, g, a.Lx, a.Ly, wbuf);
-    if (tid == 0) {
-      const long long kk = total;
-      const int rev = (int)((kk * (kk - 1) / 2) & 1);
-      float s = ((odd & 1) ^ rev) ? -1.0f : 1.0f;
-      if (total != n) s = 0.0f;  // wrong particle number: amplitude 0
-      a.item_sign[item] = s;
-    }
+    write_occupied_rows(simg, occl, wbuf, N, a.n, d, g, a.Lx, a.Ly,
+                        a.Y + (int64_t)slot * a.n * d, a.idx + (int64_t)slot * a.n,
+                        a.item_sign + item,
+                        [&](int sg, int aa, int site) { return in[(sg * d + aa) * NS + site]; });
   }
 }
 
@@ -302,6 +250,7 @@ size_t cnn_scratch_bytes(int N, int C) {
 
 int launch_cnn(const CnnLaunch& q, cudaStream_t st) {
   const nh_backflow_params& p = *q.p;
+  if (p.net == NH_NET_RESCONV) return launch_resconv(q, st);
   const int N = p.Lx * p.Ly, C = p.channels;
   if (C % 16 || C < 16 || C > 64 || p.layers < 1 || N % 2 || N > kMaxN)
     return fail(NH_ERR_UNSUPPORTED, "cnn: channels %d (multiple of 16, <= 64), layers %d, N %d",

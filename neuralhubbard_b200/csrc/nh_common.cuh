@@ -104,6 +104,70 @@ __device__ __forceinline__ int image_sign_parity(const int* simg, int g, int Lx,
                                  (int)(blockDim.x >> 5), BlockSync{});
 }
 
+// Exclusive scan of one int per thread over a kNumThreads block; returns the exclusive prefix,
+// *total the sum.  warp_buf: kNumThreads / 32 ints.
+__device__ __forceinline__ int block_scan(int v, int* warp_buf, int* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_buf[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int w = lane < (kNumThreads / 32) ? warp_buf[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < (kNumThreads / 32)) warp_buf[lane] = w;
+  }
+  __syncthreads();
+  int base = wid ? warp_buf[wid - 1] : 0;
+  *total = warp_buf[kNumThreads / 32 - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+// Mode-1 output of the backflow networks for one item, by a kNumThreads block: the ascending
+// occupied modes of the image configuration simg (+-1, 2N), the rows Y[p, a] = feat(spin, a,
+// site) of those modes (p < n), their mode indices, and the item sign eta_g(s) (-1)^(k(k-1)/2)
+// (0 for a wrong particle number k != n).  occl: 2N ints; wbuf: 4 Lx + 32 ints.
+template <typename T, typename Feat>
+__device__ void write_occupied_rows(const int* simg, int* occl, int* wbuf, int N, int n, int d,
+                                    int g, int Lx, int Ly, T* Ydst, int32_t* idst,
+                                    float* sign_dst, Feat feat) {
+  const int tid = threadIdx.x, M2 = 2 * N;
+  const int per = (M2 + kNumThreads - 1) / kNumThreads;
+  const int m0 = tid * per;
+  int cnt = 0;
+  for (int m = m0; m < m0 + per && m < M2; ++m) cnt += simg[m] > 0;
+  int total;
+  int pos = block_scan(cnt, wbuf, &total);
+  for (int m = m0; m < m0 + per && m < M2; ++m)
+    if (simg[m] > 0) occl[pos++] = m;
+  __syncthreads();
+  for (int o = tid; o < n * d; o += kNumThreads) {
+    const int p = o / d, aa = o - p * d;
+    const int m = occl[p < total ? p : 0];
+    const int sg = m >= N ? 1 : 0;
+    Ydst[o] = feat(sg, aa, m - sg * N);
+  }
+  for (int p = tid; p < n; p += kNumThreads) idst[p] = occl[p < total ? p : 0];
+  // eta_g from per-row occupation counts (closed form of the inversion parity).
+  const int odd = image_sign_parity(simg, g, Lx, Ly, wbuf);
+  if (tid == 0) {
+    const long long kk = total;
+    const int rev = (int)((kk * (kk - 1) / 2) & 1);
+    float s = ((odd & 1) ^ rev) ? -1.0f : 1.0f;
+    if (total != n) s = 0.0f;  // wrong particle number: amplitude 0
+    *sign_dst = s;
+  }
+}
+
 // ------------------------------------------------------------------ Philox4x32-10
 // Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC'11).
 struct u32x4 {
@@ -158,8 +222,8 @@ struct PipelineBuffers {
   void* cnn_act;      // large lattices: per-CTA CNN activation planes (cnn_scratch_bytes)
 };
 
-size_t pipeline_bytes(int max_items, int n, int d, int N, int C);
-PipelineBuffers carve_pipeline(void* ws, int max_items, int n, int d, int N, int C);
+size_t pipeline_bytes(int max_items, const nh_backflow_params& p);
+PipelineBuffers carve_pipeline(void* ws, int max_items, const nh_backflow_params& p);
 
 // CNN launch: all items of a configuration list (slot = item), or the items of a device list.
 struct CnnLaunch {
@@ -237,6 +301,13 @@ bool pfaffian64_fits(int n);
 bool pfaffian_needs_scratch(int n, bool fp64);
 size_t pfaffian_scratch_bytes(int n);
 size_t cnn_scratch_bytes(int N, int C);
+// Residual network (nh_resconv.cu): packed weight size, packing, forward (same CnnLaunch
+// contract as launch_cnn) and its per-CTA activation-plane scratch.
+size_t resconv_packed_floats(int channels, int blocks);
+int launch_pack_resconv(const float* conv_w, int channels, int blocks, float* packed,
+                        cudaStream_t st);
+int launch_resconv(const CnnLaunch& q, cudaStream_t st);
+size_t resconv_scratch_bytes(int N);
 
 // Full amplitude of a configuration list: CNN -> gather + Pfaffian -> image combination.
 int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const PipelineBuffers& b,

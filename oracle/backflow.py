@@ -143,7 +143,9 @@ def occupied_features(y: np.ndarray, idx: np.ndarray) -> np.ndarray:
 def amplitude(s: np.ndarray, params: dict, chunk: int = 64):
     """Unprojected (sign, logabs) of psi(s) for s (B, 2N), FP64.
 
-    ``params``: dict with conv_w, conv_b (lists), W (3, N, d), theta, Lx, Ly.
+    ``params``: dict with conv_w, conv_b (lists), W (3, N, d), theta, Lx, Ly; with
+    ``net="resconv"`` also ``embed`` (C, 4), and conv_w / conv_b hold the residual blocks'
+    convolutions (``oracle.resconv``).
     """
     Lx, Ly = params["Lx"], params["Ly"]
     Wt = build_wtilde(params["W"], params["theta"], Lx, Ly, np.float64)
@@ -151,7 +153,12 @@ def amplitude(s: np.ndarray, params: dict, chunk: int = 64):
     signs, logs = [], []
     for c0 in range(0, s.shape[0], chunk):
         sc = s[c0 : c0 + chunk]
-        y = cnn_forward(sc, params["conv_w"], params["conv_b"], Lx, Ly)
+        if params.get("net", "cnn") == "resconv":
+            from .resconv import resconv_forward
+
+            y = resconv_forward(sc, params["embed"], params["conv_w"], params["conv_b"], Lx, Ly)
+        else:
+            y = cnn_forward(sc, params["conv_w"], params["conv_b"], Lx, Ly)
         idx = fermion_idx(sc)
         Y = occupied_features(y, idx)
         F = pairing_occ(Y, idx, Wt, Lx, Ly)
