@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define NH_ABI_VERSION 5
+#define NH_ABI_VERSION 6
 
 enum {
   NH_OK = 0,
@@ -69,9 +69,11 @@ enum {
  *                down, d = channels / 2.
  * conv_w_packed: the same weights repacked by nh_pack_cnn_weights (NH_NET_CNN) or
  *                nh_pack_resconv_weights (NH_NET_RESCONV, 16-byte aligned); read by the kernels.
- * conv_w_tc:     BF16 hi/lo tensor-core layout from nh_pack_cnn_weights_tc (cnn_mode 1 and 2).
  * cnn_mode:      0 = FP32 CUDA cores; 1 = tcgen05 BF16; 2 = tcgen05 BF16 x3 (hi*hi + hi*lo +
- *                lo*hi, near-FP32).  Modes 1 and 2 need a 16x16 lattice, 32 channels, 4 layers.
+ *                lo*hi, near-FP32).  NH_NET_CNN: modes 1 and 2 need a 16x16 lattice, 32 channels,
+ *                4 layers.  NH_NET_RESCONV: modes 0 and 2, mode 2 on a 16x16 lattice.
+ * conv_w_tc:     BF16 hi/lo tensor-core image from nh_pack_cnn_weights_tc (NH_NET_CNN) or
+ *                nh_pack_resconv_weights_tc (NH_NET_RESCONV); 16-byte aligned.
  * pf_mode:       0 = Pfaffian on CUDA cores (two matrices per SM in shared memory); 1 = matrix
  *                resident in tensor memory, rank-16 trailing updates as 3xTF32 tcgen05 MMAs
  *                (one matrix per SM).  The FP64 recompute always uses the CUDA-core kernel.
@@ -148,7 +150,8 @@ enum {
   NH_K_PROP_ADAM = 21,
   NH_K_RESCONV = 22,
   NH_K_RESCONV64 = 23,
-  NH_K_COUNT = 24
+  NH_K_RESCONV_TC = 24,
+  NH_K_COUNT = 32
 };
 int nh_profile_enable(int on);
 int nh_profile_read(double* ms, int64_t* launches, int n_ids);
@@ -167,6 +170,11 @@ int nh_pack_cnn_weights(const float* conv_w, int channels, int layers, float* pa
 size_t nh_pack_resconv_weights_floats(int channels, int blocks);
 int nh_pack_resconv_weights(const float* conv_w, int channels, int blocks, float* packed,
                             void* stream);
+/* Residual network, tensor-core image (nh_pack_resconv_weights_tc_bytes(blocks) bytes): per
+ * convolution and tap the BF16 hi and lo weights in the K-major core-matrix layout; 64 channels. */
+size_t nh_pack_resconv_weights_tc_bytes(int blocks);
+int nh_pack_resconv_weights_tc(const float* conv_w, int channels, int blocks, void* packed,
+                               void* stream);
 
 /* Tensor-core weight image (nh_pack_cnn_weights_tc_bytes() bytes): BF16 hi and lo parts in the
  * K-major core-matrix layout; 32 channels, 4 layers. */

@@ -73,6 +73,8 @@ SIGNATURES = {
     "nh_pack_cnn_weights": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "nh_pack_resconv_weights_floats": (c_size_t, [c_int, c_int]),
     "nh_pack_resconv_weights": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
+    "nh_pack_resconv_weights_tc_bytes": (c_size_t, [c_int]),
+    "nh_pack_resconv_weights_tc": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "nh_pack_cnn_weights_tc_bytes": (c_size_t, []),
     "nh_pack_cnn_weights_tc": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
     "nh_cnn_forward": (c_int, [c_void_p, c_int, P_BF, c_void_p, c_void_p]),
@@ -146,9 +148,9 @@ KERNEL_IDS = {
     "hop_emit": 6, "eloc_reduce": 7, "mh_propose": 8, "compact": 9, "mh_accept": 10,
     "wtilde": 11, "pfaffian64": 12, "cnn64": 13, "flagged": 14, "pack": 15, "cnn_tc": 16,
     "pfaffian_tc": 17, "prop_sample": 18, "prop_forward": 19, "prop_backward": 20,
-    "prop_adam": 21, "resconv": 22, "resconv64": 23,
+    "prop_adam": 21, "resconv": 22, "resconv64": 23, "resconv_tc": 24,
 }
-K_COUNT = 24
+K_COUNT = 32
 
 
 def profile_enable(on: bool) -> None:

@@ -193,6 +193,11 @@ class PfaffianBackflow:
             _lib.call("nh_pack_cnn_weights", self.conv_w.data_ptr(), self.channels,
                       self.layers, self.conv_w_packed.data_ptr(), stream_ptr(dev))
         self.conv_w_tc = None
+        if self.net == _lib.NET_RESCONV and self.geom.LX == 16 and self.geom.LY == 16:
+            nbytes = _lib.load().nh_pack_resconv_weights_tc_bytes(self.layers)
+            self.conv_w_tc = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            _lib.call("nh_pack_resconv_weights_tc", self.conv_w.data_ptr(), self.channels,
+                      self.layers, self.conv_w_tc.data_ptr(), stream_ptr(dev))
         if self.net == _lib.NET_CNN and self.channels == 32 and self.layers == 4:
             nbytes = _lib.load().nh_pack_cnn_weights_tc_bytes()
             self.conv_w_tc = torch.empty(nbytes, dtype=torch.uint8, device=dev)

@@ -148,7 +148,9 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
   if (p.cnn_mode == 1 || p.cnn_mode == 2 || p.pf_mode == 1)
     if ((rc = check_cuda(cudaMemsetAsync(b.err, 0, sizeof(int32_t), st), "clear error word")))
       return rc;
-  if (p.cnn_mode == 1 || p.cnn_mode == 2) {
+  if (p.net == NH_NET_RESCONV && p.cnn_mode == 2) {
+    rc = launch_resconv_tc(cl, p, b.Y, b.idx, b.item_sign, b.err, st);
+  } else if (p.cnn_mode == 1 || p.cnn_mode == 2) {
     rc = launch_cnn_tc(cl, p, p.cnn_mode, b.Y, b.idx, b.item_sign, b.err, st);
   } else {
     CnnLaunch c{&cl, &p, 1, false, nullptr, nullptr, 0, nullptr, b.Y, b.idx, b.item_sign,
@@ -195,12 +197,15 @@ static int check_params(const nh_backflow_params* p) {
   if (p->layers < 1 || p->layers > 16) return fail(NH_ERR_UNSUPPORTED, "layers %d", p->layers);
   if (p->net != NH_NET_CNN && p->net != NH_NET_RESCONV)
     return fail(NH_ERR_INVALID, "net %d (NH_NET_CNN or NH_NET_RESCONV)", p->net);
-  if (p->net == NH_NET_RESCONV && (p->channels != 64 || p->cnn_mode != 0))
-    return fail(NH_ERR_UNSUPPORTED, "the residual network needs 64 channels and cnn_mode 0");
   if (p->cnn_mode < 0 || p->cnn_mode > 2) return fail(NH_ERR_INVALID, "cnn_mode %d", p->cnn_mode);
-  if (p->cnn_mode && !cnn_tc_supported(*p))
+  if (p->net == NH_NET_RESCONV) {
+    if (p->channels != 64 || p->cnn_mode == 1 || (p->cnn_mode == 2 && !resconv_tc_supported(*p)))
+      return fail(NH_ERR_UNSUPPORTED, "the residual network needs 64 channels and cnn_mode 0, "
+                  "or cnn_mode 2 on a 16x16 lattice");
+  } else if (p->cnn_mode && !cnn_tc_supported(*p)) {
     return fail(NH_ERR_UNSUPPORTED, "cnn_mode %d needs a 16x16 lattice, 32 channels, 4 layers",
                 p->cnn_mode);
+  }
   if (p->cnn_mode && !p->conv_w_tc) return fail(NH_ERR_INVALID, "cnn_mode %d: conv_w_tc is null",
                                                 p->cnn_mode);
   if (p->pf_mode < 0 || p->pf_mode > 1) return fail(NH_ERR_INVALID, "pf_mode %d", p->pf_mode);
@@ -278,6 +283,19 @@ int nh_pack_resconv_weights(const float* conv_w, int channels, int blocks, float
   if (channels != 64)
     return fail(NH_ERR_UNSUPPORTED, "pack_resconv_weights: %d channels (64)", channels);
   return launch_pack_resconv(conv_w, channels, blocks, packed, static_cast<cudaStream_t>(stream));
+}
+
+size_t nh_pack_resconv_weights_tc_bytes(int blocks) {
+  return blocks > 0 ? resconv_tc_packed_bytes(blocks) : 0;
+}
+
+int nh_pack_resconv_weights_tc(const float* conv_w, int channels, int blocks, void* packed,
+                               void* stream) {
+  if (!conv_w || !packed || blocks < 1)
+    return fail(NH_ERR_INVALID, "pack_resconv_weights_tc: bad arguments");
+  if (channels != 64)
+    return fail(NH_ERR_UNSUPPORTED, "pack_resconv_weights_tc: %d channels (64)", channels);
+  return launch_pack_resconv_tc(conv_w, blocks, packed, static_cast<cudaStream_t>(stream));
 }
 
 size_t nh_pack_cnn_weights_tc_bytes(void) { return cnn_tc_packed_bytes(); }

@@ -36,15 +36,15 @@
 #include <cuda_bf16.h>
 
 #include "nh_common.cuh"
+#include "nh_tcgen05.cuh"
 
 namespace nh {
 namespace {
 
+using namespace tc;
+
 constexpr int kTcThreads = 256;
 constexpr int kC = 32;          // channels
-constexpr int kL = 16;          // lattice extent handled by this kernel
-constexpr int kP = kL + 2;      // padded extent
-constexpr int kPlane = kP * kP * 16;             // bytes of one 8-channel plane
 constexpr int kW0Bytes = 2 * 9 * 2 * 4 * 128;    // layer 0: q x tap x kc(2) x cg(4) x 128 B
 constexpr int kW1Bytes = 2 * 9 * 4 * 4 * 128;    // layers 1..3: q x tap x kc(4) x cg(4) x 128 B
 constexpr int kWBytes = kW0Bytes + 3 * kW1Bytes;
@@ -53,7 +53,6 @@ constexpr int kWG = 2;                           // independent warp groups per 
 constexpr int kWGThreads = kTcThreads / kWG;     // 128
 constexpr int kIntsPerWG = 3 * 2 * kL * kL + 4 * kL + 32;  // simg, rowof, occl, scan scratch
 constexpr unsigned kTmemCols = 64 * kWG;         // two 128 x 32 FP32 accumulators per group
-constexpr long long kWaitLimit = 1ll << 22;      // mbarrier polls before giving up
 
 struct TcArgs {
   ConfigList cl;
@@ -67,103 +66,14 @@ struct TcArgs {
   int32_t* err;         // error word (0 = ok)
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// K-major, no-swizzle shared-memory matrix descriptor (tcgen05 layout, version 1).
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
-  return d;                // base offset 0, legacy LBO mode, SWIZZLE_NONE
-}
-
 // Instruction descriptor: kind::f16, BF16 x BF16 -> FP32, both K-major, M = 128, N = 32.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) |
-                            ((128u >> 4) << 24);
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, bool acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(kIdesc), "r"((uint32_t)acc));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (long long it = 0; it < kWaitLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
-      "%30, %31}, [%32];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
+constexpr uint32_t kIdesc = idesc_bf16(128, 32);
 
 // tanh-approximated GELU written as x * sigmoid(2 z), z = sqrt(2/pi) (x + 0.044715 x^3), which is
 // the same function as 0.5 x (1 + tanh z); the exponential is the fast __expf intrinsic.
 __device__ __forceinline__ float gelu_tanh(float x) {
   const float z2 = 1.5957691216057308f * (x + 0.044715f * x * x * x);
   return __fdividef(x, 1.0f + __expf(-z2));
-}
-
-__device__ __forceinline__ uint16_t bf16_bits(float x) {
-  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
-}
-__device__ __forceinline__ float bf16_val(uint16_t b) {
-  return __bfloat162float(__ushort_as_bfloat16(b));
-}
-
-// Padded position of lattice site (x, y) shifted by (ox, oy) in {-1, 0, 1}: byte offset.
-__device__ __forceinline__ int pad_off(int X, int Y) { return (X * kP + Y) * 16; }
-
-// Write the 8-channel groups of one site (and its periodic halo copies) into the planes.
-__device__ __forceinline__ void put_site(unsigned char* planes, int nplanes, int x, int y,
-                                         const uint4* grp) {
-  const int xs[2] = {x + 1, x == 0 ? kL + 1 : (x == kL - 1 ? 0 : -1)};
-  const int ys[2] = {y + 1, y == 0 ? kL + 1 : (y == kL - 1 ? 0 : -1)};
-#pragma unroll
-  for (int a = 0; a < 2; ++a) {
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      if (xs[a] < 0 || ys[b] < 0) continue;
-      const int off = pad_off(xs[a], ys[b]);
-      for (int kc = 0; kc < nplanes; ++kc)
-        *reinterpret_cast<uint4*>(planes + kc * kPlane + off) = grp[kc];
-    }
-  }
 }
 
 // Issue the MMAs of one layer for both tiles (one thread).
@@ -189,10 +99,10 @@ __device__ void issue_layer(uint32_t tmem, uint32_t act_hi, uint32_t act_lo, uin
         const uint32_t bo = tap * tap_bytes + 2 * kh * 4 * 128;
         const uint64_t ahi = make_desc(act_hi + ao, lbo_a, sbo_a);
         const uint64_t bhi = make_desc(w_hi + bo, lbo_b, sbo_b);
-        mma_bf16(d, ahi, bhi, acc);
+        mma_bf16(d, ahi, bhi, kIdesc, acc);
         acc = true;
-        if (split_w) mma_bf16(d, ahi, make_desc(w_lo + bo, lbo_b, sbo_b), true);
-        if (split_act) mma_bf16(d, make_desc(act_lo + ao, lbo_a, sbo_a), bhi, true);
+        if (split_w) mma_bf16(d, ahi, make_desc(w_lo + bo, lbo_b, sbo_b), kIdesc, true);
+        if (split_act) mma_bf16(d, make_desc(act_lo + ao, lbo_a, sbo_a), bhi, kIdesc, true);
       }
     }
   }

@@ -308,6 +308,12 @@ int launch_pack_resconv(const float* conv_w, int channels, int blocks, float* pa
                         cudaStream_t st);
 int launch_resconv(const CnnLaunch& q, cudaStream_t st);
 size_t resconv_scratch_bytes(int N);
+// Residual network on the tensor cores (nh_resconv_tc.cu): 16x16, 64 channels, BF16 x3.
+size_t resconv_tc_packed_bytes(int blocks);
+bool resconv_tc_supported(const nh_backflow_params& p);
+int launch_pack_resconv_tc(const float* conv_w, int blocks, void* packed, cudaStream_t st);
+int launch_resconv_tc(const ConfigList& cl, const nh_backflow_params& p, float* Y, int32_t* idx,
+                      float* item_sign, int32_t* err, cudaStream_t st);
 
 // Full amplitude of a configuration list: CNN -> gather + Pfaffian -> image combination.
 int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const PipelineBuffers& b,

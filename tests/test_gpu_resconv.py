@@ -127,3 +127,33 @@ def test_released_state_energy():
     var = e.var(ddof=1) * 256
     assert abs(mean - info.energy) < 4 * err, (mean, err)
     assert 0.5 * info.variance < var < 1.5 * info.variance, var
+
+
+@pytest.mark.parametrize("blocks", [1, 3])
+def test_resconv_tc_amplitude(blocks):
+    """16x16 on the tensor cores (cnn_mode 2, BF16 x3 products): signs exact; without any FP64
+    recompute log|psi| within 2e-3 of the FP64 oracle, with the default recompute within 1e-3."""
+    L, N = 16, 256
+    ne = 7 * N // 16
+    params = random_resconv(L, blocks, seed=30 + blocks)
+    s = olat.random_configs(np.random.default_rng(40 + blocks), 4, N, ne, ne)
+    for symm, kw, tol in [(False, dict(cond_tau=0.0, cancel_tau=0.0), 2e-3), (True, {}, 1e-3)]:
+        s0, l0 = oproj.projected_amplitude(s, oracle_params(params, L), symm=symm)
+        model = nh.PfaffianBackflow(L, L, ne, ne, params=params, cnn_mode=2, **kw)
+        sg, la = nh.Variational(model, symm=symm)(s).numpy()
+        assert np.array_equal(sg, s0)
+        assert np.max(np.abs(la - l0)) < tol, (symm, np.max(np.abs(la - l0)))
+
+
+def test_released_state_energy_tensor_cores():
+    """The tensor-core network (cnn_mode 2) gives the released state's E/N on 256 stored chains
+    within 4 standard errors of the published value as well."""
+    params, spins = released()
+    info = checkpoint.RELEASED[NAME]
+    ne = 7 * 256 // 16
+    state = nh.Variational(nh.PfaffianBackflow(16, 16, ne, ne, params=params, cnn_mode=2))
+    H = nh.Hubbard(8.0, [1.0, info.tprime], [1, 2])
+    s = torch.from_numpy(spins[256:512]).to(DEV)
+    e = H.Oloc(state, nh.Samples(s, state(s))).cpu().numpy() / 256
+    mean, err = e.mean(), e.std(ddof=1) / np.sqrt(len(e))
+    assert abs(mean - info.energy) < 4 * err, (mean, err)
