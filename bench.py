@@ -20,6 +20,8 @@ ragged local energy at 8x8, 16x16 and 24x24, one CUDA-graph replay each; ``large
 (1 GPU) times Metropolis steps at 32x32 (n = 896) with the uniform hop and the learned proposal.
 ``precision`` (1 GPU) reports each precision form's |delta log|psi_P|| and sign mismatches
 against the library's all-FP64 path, and near-nodal log-Pfaffians at the slogpf boundary.
+``resconv`` (1 GPU) times the released states' residual network (16 blocks x 64 channels) on
+CUDA cores and on the tensor cores, with E/N of the released 16x16 state on 512 of its chains.
 
 Under torchrun each rank evaluates its own 8192 configurations (weak scaling); the time is the
 maximum over ranks of the summed per-step CUDA-event durations.  ``--impl reference`` times the
@@ -509,6 +511,80 @@ def measure_large(args, dev, st, q) -> dict:
     return out
 
 
+def measure_resconv(args, dev, st) -> dict:
+    """The released states' residual network (16 blocks x 64 channels, d = 32) at 16x16: projected
+    amplitudes of 1024 configurations x 8 images on CUDA cores (FP32) and on the tensor cores
+    (BF16 x3), each against the all-FP64 path; with the released tpm02_L16_pfaffian weights
+    (tests/golden/released/, copied by tests/golden/fetch_released.py) the configurations are
+    its stored chains and E/N on 512 of them is measured with the tensor-core form."""
+    import torch
+
+    import neuralhubbard_b200 as nh
+    from neuralhubbard_b200 import _lib, checkpoint
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    eqx = os.path.join(here, "tests", "golden", "released", "tpm02_L16_pfaffian.eqx")
+    ne = 7 * N_SITES // 16
+    released = os.path.exists(eqx)
+    if released:
+        params = checkpoint.load_pfaffian_backflow(eqx, L)
+        spins = checkpoint.load_spins(eqx.replace(".eqx", "_spins.npz"), N_SITES)
+    else:
+        rng = np.random.default_rng(61)
+        params = dict(net="resconv", embed=rng.normal(size=(64, 4)).astype(np.float32),
+                      conv_w=[(rng.normal(size=(64, 64, 3, 3)) * 0.04).astype(np.float32)
+                              for _ in range(32)],
+                      conv_b=[(rng.normal(size=64) * 0.1).astype(np.float32) for _ in range(32)],
+                      W=(rng.normal(size=(3, N_SITES, 32)) / np.sqrt(32)).astype(np.float32),
+                      theta=0.55)
+        spins = nh.random_spins(np.random.default_rng(62), 1024, N_SITES, ne, ne)
+    B = 1024
+    s = torch.from_numpy(spins[:B]).to(dev)
+    ref = nh.Variational(nh.PfaffianBackflow(L, L, ne, ne, params=params, cond_tau=1.0,
+                                             device=dev))(s)
+    out = {"weights": "released tpm02_L16_pfaffian" if released else "random (LeCun-sized)",
+           "network": "16 residual blocks x 64 channels, d = 32 (code/backflow/models.py:319-329)",
+           "configurations": B, "images": IMAGES,
+           "reference_a100_us_per_amplitude": {
+               "cnn_tf32": 16.0, "pfaffian_3xtf32_n256": 3.39,
+               "source": "data/supplement/tableS3_amplitude_cost/amplitude_cost.csv rows "
+                         "'16,256,Normal CNN' and '16,256,Pfaffian' (A100, half filling)"}}
+    for name, mode in (("cuda_cores_fp32", 0), ("tensor_cores_bf16x3", 2)):
+        state = nh.Variational(nh.PfaffianBackflow(L, L, ne, ne, params=params, cnn_mode=mode,
+                                                   device=dev))
+        for _ in range(2):
+            state(s)
+        torch.cuda.synchronize()
+        _lib.profile_enable(True)
+        _lib.profile_read()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        psi = state(s)
+        e1.record(st)
+        torch.cuda.synchronize()
+        kern = _lib.profile_read()
+        _lib.profile_enable(False)
+        d = (psi.logabs - ref.logabs).abs().cpu().numpy()
+        out[name] = {"amplitudes_per_s": B * IMAGES / (e0.elapsed_time(e1) / 1e3),
+                     "kernels_ms": {k: v[0] for k, v in kern.items()},
+                     "max_abs_dlog": float(d.max()), "mean_abs_dlog": float(d.mean()),
+                     "sign_mismatches": int((psi.sign != ref.sign).sum().item())}
+    if released:
+        info = checkpoint.RELEASED["tpm02_L16_pfaffian"]
+        state = nh.Variational(nh.PfaffianBackflow(L, L, ne, ne, params=params, cnn_mode=2,
+                                                   device=dev))
+        H = nh.Hubbard(8.0, [1.0, info.tprime], [1, 2])
+        sc = torch.from_numpy(spins[1024:1536]).to(dev)
+        t0 = time.time()
+        e = H.Oloc(state, nh.Samples(sc, state(sc))).cpu().numpy() / N_SITES
+        out["energy"] = {"chains": 512, "E_per_site": float(e.mean()),
+                         "E_per_site_err": float(e.std(ddof=1) / math.sqrt(len(e))),
+                         "published": info.energy, "published_err": info.energy_err,
+                         "seconds": time.time() - t0}
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -624,6 +700,9 @@ def run_ours(args) -> None:
     precision = None
     if world == 1 and not args.no_precision:
         precision = measure_precision(dev, st, spins, flush)
+    resconv = None
+    if world == 1 and not args.no_resconv:
+        resconv = measure_resconv(args, dev, st)
 
     if rank == 0:
         cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
@@ -650,6 +729,7 @@ def run_ours(args) -> None:
             "local_energy": local_energy,
             "large_lattice": large,
             "precision": precision,
+            "resconv": resconv,
             "roofline": roof, "kernels": kernels, "gpu_launches": launches,
             "cpu_baseline": cpu, "clocks": clk,
         }
@@ -707,6 +787,8 @@ def main():
                     help="skip the 32x32 (n = 896) Metropolis measurement")
     ap.add_argument("--large-chains", type=int, default=4096)
     ap.add_argument("--large-steps", type=int, default=2)
+    ap.add_argument("--no-resconv", action="store_true",
+                    help="skip the released-state residual network block")
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the precision-form report (errors against the all-FP64 path)")
     ap.add_argument("--chains", type=int, default=1024)

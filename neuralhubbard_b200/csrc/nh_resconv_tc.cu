@@ -3,9 +3,11 @@
 //
 // Each 3x3 periodic convolution is an implicit GEMM D[site, co] += A[site + tap, ci] W[tap][ci, co]
 // on tcgen05: M = 128 (two tiles, y-blocks 0-7 and 8-15, of 16 x-rows), N = 64 output channels,
-// K = 16 input channels per MMA, FP32 accumulators in 128 tensor-memory columns.  Operands are
-// split into BF16 hi + lo and accumulated as hi*hi + hi*lo + lo*hi (about 16 significant bits
-// per product).  One configuration image per CTA at a time (grid-stride), 256 threads: warp w
+// K = 16 input channels per MMA, FP32 accumulators in tensor memory: four partial sums per tile
+// (one per group of 16 input channels, 512 columns), added in the epilogue, which keeps the
+// tensor cores' FP32 accumulation chains short (one chain of 216 MMAs left a nearly constant
+// offset of ~8e-4 in log|psi|; four chains, under 2e-4).  Operands are split into BF16 hi + lo
+// and accumulated as hi*hi + hi*lo + lo*hi (about 16 significant bits per product).  One configuration image per CTA at a time (grid-stride), 256 threads: warp w
 // owns tensor-memory lanes 32 (w % 4) .. + 31 of tile w / 4, i.e. one site per thread.
 //
 // Shared memory (214 KB):
@@ -16,8 +18,10 @@
 //   ring    4 slots of one tap's weights (hi + lo, 16 KB, [q][kc][cg][8 co][8 ci] BF16), filled
 //           by bulk copies (no multicast) that complete on full[slot]; the MMAs that read a slot
 //           commit to empty[slot], and the copy of the slice four taps ahead waits for it.
-// Thread 0 issues the copies and the MMAs; the weight stream runs ahead across convolutions,
-// so the next convolution's first slices load while the epilogue of the current one runs.
+// Thread 0 issues the MMAs (all 216 of a convolution unrolled, operand descriptors formed once
+// and advanced by constants); thread 32 issues the copies, so that neither waits on the other's
+// instructions.  The weight stream runs ahead across convolutions: the next convolution's first
+// four slices load while the epilogue of the current one runs.
 // Epilogues read the accumulators with tcgen05.ld and (a) write u's planes, or (b) add the
 // convolution into x, reduce sum x^2 over the CTA, and write the next h's planes.
 //
@@ -46,7 +50,8 @@ constexpr int kRtConvBytes = 9 * kRtTapBytes;          // 147,456
 constexpr int kRtSlots = 4;
 constexpr int kRtInts = 2 * kRtN + 2 * kRtN + 4 * kL + 32;  // simg, occl, scan scratch
 constexpr uint32_t kRtIdesc = idesc_bf16(128, 64);
-constexpr unsigned kRtTmemCols = 128;
+constexpr int kRtParts = 4;           // partial accumulators per tile (one per 16-ci group)
+constexpr unsigned kRtTmemCols = 128 * kRtParts;
 constexpr float kRtRmsEps = 1e-6f;
 
 constexpr size_t kOffX = kRtActBytes;
@@ -54,7 +59,8 @@ constexpr size_t kOffRing = kOffX + kRtXBytes;
 constexpr size_t kOffInts = kOffRing + (size_t)kRtSlots * kRtTapBytes;
 constexpr size_t kOffRed = kOffInts + sizeof(int) * kRtInts;
 constexpr size_t kOffBars = (kOffRed + 8 * sizeof(float) + 7) & ~(size_t)7;
-constexpr size_t kRtSmem = kOffBars + (2 * kRtSlots + 1) * 8 + 16;
+constexpr size_t kRtSmem = kOffBars + (2 * kRtSlots + 1) * 8 + 16;  // + tmem slot, flag, count
+static_assert((kOffBars + (2 * kRtSlots + 1) * 8 + 8) % 8 == 0, "8-byte slot for the count");
 static_assert(kOffX % 128 == 0 && kOffRing % 128 == 0, "operand regions 128-byte aligned");
 static_assert(kRtSmem <= 227 * 1024, "resident set must fit in shared memory");
 
@@ -75,23 +81,26 @@ __device__ __forceinline__ float gelu_fast(float x) {
   return __fdividef(x, 1.0f + __expf(-z2));
 }
 
-// Thread 0: the MMAs of one tap for both tiles from ring slot address wb.
-__device__ __forceinline__ void issue_tap(uint32_t tmem, uint32_t act_hi, uint32_t act_lo,
-                                          uint32_t wb, int tap) {
+// Thread 0: the MMAs of one tap for both tiles.  dAhi / dAlo / dB are the descriptors of the hi
+// planes, the lo planes and the tap's ring slot; with the tap known at compile time (the caller
+// unrolls) every operand is that descriptor plus a constant (its address field counts 16-byte
+// units; shared-memory offsets stay far below the field's 256 KB range).  Input-channel group kk
+// accumulates into its own partial sum (columns 128 kk + 64 h), so each FP32 accumulation chain
+// is a quarter as long; the epilogue adds the four.
+__device__ __forceinline__ void issue_tap(uint32_t tmem, uint64_t dAhi, uint64_t dAlo,
+                                          uint64_t dB, int tap) {
   const int dx = tap / 3 - 1, dy = tap % 3 - 1;
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const uint32_t d = tmem + 64 * h;
-    const uint32_t aoff = (uint32_t)pad_off(dx + 1, 8 * h + dy + 1);
+  for (int q = 0; q < 3; ++q) {  // hi*hi, hi*lo, lo*hi
 #pragma unroll
-    for (int kk = 0; kk < kRtPlanes / 2; ++kk) {
-      const uint32_t ao = aoff + 2 * kk * kPlane;
-      const uint32_t bo = 2 * kk * (kRtPlanes * 128);
-      const uint64_t ahi = make_desc(act_hi + ao, kPlane, kP * 16);
-      const uint64_t bhi = make_desc(wb + bo, kRtPlanes * 128, 128);
-      mma_bf16(d, ahi, bhi, kRtIdesc, tap > 0 || kk > 0);
-      mma_bf16(d, ahi, make_desc(wb + kRtHalfTap + bo, kRtPlanes * 128, 128), kRtIdesc, true);
-      mma_bf16(d, make_desc(act_lo + ao, kPlane, kP * 16), bhi, kRtIdesc, true);
+    for (int kk = 0; kk < kRtParts; ++kk) {
+      const uint64_t b = dB + (uint64_t)(((q == 1 ? kRtHalfTap : 0) + 2 * kk * kRtPlanes * 128) >> 4);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const uint32_t ao = (uint32_t)pad_off(dx + 1, 8 * h + dy + 1) + 2 * kk * kPlane;
+        const uint64_t a = (q == 2 ? dAlo : dAhi) + (uint64_t)(ao >> 4);
+        mma_bf16(tmem + 128 * kk + 64 * h, a, b, kRtIdesc, tap > 0 || q > 0);
+      }
     }
   }
 }
@@ -119,6 +128,7 @@ __global__ void __launch_bounds__(kRtThreads, 1) resconv_tc_kernel(RtArgs a) {
   uint64_t* accb = empty + kRtSlots;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accb + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+  long long* consumed_total = reinterpret_cast<long long*>(abort_flag + 1);  // at kOffBars + 80
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int quarter = warp & 3, tile = warp >> 2;
@@ -133,9 +143,11 @@ __global__ void __launch_bounds__(kRtThreads, 1) resconv_tc_kernel(RtArgs a) {
                                 : 0;
   const int convs = 2 * a.blocks;
   const long long slices = (long long)my_items * convs * 9;  // weight slices this CTA uses
-  long long loaded = 0, consumed = 0;                        // thread 0's stream position
+  constexpr int kProducer = 32;                              // thread issuing the copies
+  long long loaded = 0;    // slices requested (producer thread)
+  long long consumed = 0;  // slices whose MMAs are issued (thread 0)
 
-  auto load_slice = [&](long long sidx) {  // thread 0
+  auto load_slice = [&](long long sidx) {  // one thread
     const int slot = (int)(sidx % kRtSlots);
     const int conv = (int)((sidx / 9) % convs), tap = (int)(sidx % 9);
     bulk_load(ring + slot * kRtTapBytes,
@@ -151,8 +163,9 @@ __global__ void __launch_bounds__(kRtThreads, 1) resconv_tc_kernel(RtArgs a) {
     mbar_init(accb, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    for (; loaded < kRtSlots && loaded < slices; ++loaded) load_slice(loaded);
+    for (long long sl = 0; sl < kRtSlots && sl < slices; ++sl) load_slice(sl);
   }
+  loaded = slices < kRtSlots ? slices : kRtSlots;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
@@ -167,9 +180,13 @@ __global__ void __launch_bounds__(kRtThreads, 1) resconv_tc_kernel(RtArgs a) {
   const uint32_t t_lane = tmem + ((uint32_t)(32 * quarter) << 16) + 64u * tile;
   const uint32_t act_hi = smem_u32(planes), act_lo = act_hi + kRtPlanes * kPlane;
   const uint32_t ring0 = smem_u32(ring);
+  const uint64_t dAhi = make_desc(act_hi, kPlane, kP * 16);
+  const uint64_t dAlo = make_desc(act_lo, kPlane, kP * 16);
+  const uint64_t dB0 = make_desc(ring0, kRtPlanes * 128, 128);
   const float out_scale = 1.0f / sqrtf((float)(a.blocks + 1));
   const float inv_cn = 1.0f / (float)(kRtC * kRtN);
   uint32_t acc_phase = 0;
+  long long conv_seq = 0;  // convolutions processed by this CTA (all threads)
 
   // Writes h = GELU(RMSNorm(x)) of this thread's site into the planes (all threads call).
   auto norm_to_planes = [&]() {
@@ -220,8 +237,9 @@ __global__ void __launch_bounds__(kRtThreads, 1) resconv_tc_kernel(RtArgs a) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncthreads();  // planes written, accumulators read
-      if (tid == 0) {
+      if (tid == 0) {  // MMA issue: wait for each tap's weights, then its 72 MMAs
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
         for (int tap = 0; tap < 9; ++tap) {
           const int slot = (int)(consumed % kRtSlots);
           if (!*abort_flag && !mbar_wait(full + slot, (uint32_t)((consumed / kRtSlots) & 1))) {
@@ -229,23 +247,27 @@ __global__ void __launch_bounds__(kRtThreads, 1) resconv_tc_kernel(RtArgs a) {
             *abort_flag = 1;
           }
           if (*abort_flag) break;
-          issue_tap(tmem, act_hi, act_lo, ring0 + slot * kRtTapBytes, tap);
+          issue_tap(tmem, dAhi, dAlo, dB0 + (uint64_t)((slot * kRtTapBytes) >> 4), tap);
           mma_commit(empty + slot);
-          // Refill the previous slice's slot with the slice kRtSlots - 1 ahead of this one.
-          if (consumed >= 1 && loaded < slices) {
-            const long long prev = consumed - 1;
-            if (!mbar_wait(empty + (prev % kRtSlots), (uint32_t)((prev / kRtSlots) & 1))) {
-              atomicExch(a.err, 3);
-              *abort_flag = 1;
-            } else {
-              load_slice(loaded);
-              ++loaded;
-            }
-          }
           ++consumed;
         }
         mma_commit(accb);  // arrives once every MMA issued so far has completed
+      } else if (tid == kProducer) {
+        // Copies: every slice up to the fourth of the next convolution, each into the slot of
+        // the slice four back once that slice's MMAs (all of this convolution) have completed.
+        const long long upto = (long long)9 * (conv_seq + 1) + kRtSlots;
+        while (!*abort_flag && loaded < slices && loaded < upto) {
+          const long long prev = loaded - kRtSlots;
+          if (!mbar_wait(empty + (prev % kRtSlots), (uint32_t)((prev / kRtSlots) & 1))) {
+            atomicExch(a.err, 3);
+            *abort_flag = 1;
+            break;
+          }
+          load_slice(loaded);
+          ++loaded;
+        }
       }
+      ++conv_seq;
       if (!mbar_wait(accb, acc_phase)) {
         if (tid == 0) atomicExch(a.err, 4);
         *abort_flag = 1;
@@ -260,6 +282,16 @@ __global__ void __launch_bounds__(kRtThreads, 1) resconv_tc_kernel(RtArgs a) {
       float v[kRtC];
       tmem_ld32(t_lane, v);
       tmem_ld32(t_lane + 32, v + 32);
+#pragma unroll
+      for (int pc = 1; pc < kRtParts; ++pc) {
+        float w[32];
+        tmem_ld32(t_lane + 128 * pc, w);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[i] += w[i];
+        tmem_ld32(t_lane + 128 * pc + 32, w);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) v[32 + i] += w[i];
+      }
       const float* b = a.bias + conv * kRtC;
       if ((conv & 1) == 0) {  // u = GELU(Conv1(h) + b1) into the planes (h is no longer read)
 #pragma unroll
@@ -286,8 +318,10 @@ __global__ void __launch_bounds__(kRtThreads, 1) resconv_tc_kernel(RtArgs a) {
                         });
   }
   // Copies still in flight (only after an abort): wait for them, bounded, before exiting.
-  if (tid == 0) {
-    for (long long s = consumed; s < loaded; ++s)
+  if (tid == 0) *consumed_total = consumed;
+  __syncthreads();
+  if (tid == kProducer) {
+    for (long long s = *consumed_total; s < loaded; ++s)
       mbar_wait(full + (s % kRtSlots), (uint32_t)((s / kRtSlots) & 1));
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
