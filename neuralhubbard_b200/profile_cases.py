@@ -12,6 +12,8 @@ cases:
   eloc               local energy, 8x8 unprojected, 32768 configurations (8.4M connections)
   proposal_sample    learned-proposal draw, 16x16, 4096 chains
   proposal_backward  learned-proposal loss and gradient, 16x16, 4096 records
+  resconv_tc         residual network (16 blocks x 64 channels) on tcgen05, 16x16, 64 x 8 images
+  resconv            the same network on CUDA cores (FP32)
 """
 
 from __future__ import annotations
@@ -86,8 +88,35 @@ def case_proposal_backward(repeat):
         q.loss_grad(s, m.to(torch.int32), w)
 
 
+def _resconv(repeat, cnn_mode):
+    rng = np.random.default_rng(6)
+    L, C = 16, 64
+    params = dict(net="resconv", embed=rng.normal(size=(C, 4)).astype(np.float32),
+                  conv_w=[(rng.normal(size=(C, C, 3, 3)) * 0.04).astype(np.float32)
+                          for _ in range(32)],
+                  conv_b=[(rng.normal(size=C) * 0.1).astype(np.float32) for _ in range(32)],
+                  W=(rng.normal(size=(3, L * L, 32)) / np.sqrt(32)).astype(np.float32),
+                  theta=0.55)
+    ne = 7 * L * L // 16
+    model = PfaffianBackflow(L, L, ne, ne, params=params, cnn_mode=cnn_mode, cond_tau=0.0,
+                             cancel_tau=0.0)
+    state = Variational(model, symm=True)
+    s = torch.from_numpy(random_spins(np.random.default_rng(7), 64, L * L, ne, ne)).cuda()
+    for _ in range(repeat):
+        state(s)
+
+
+def case_resconv_tc(repeat):
+    _resconv(repeat, 2)
+
+
+def case_resconv(repeat):
+    _resconv(repeat, 0)
+
+
 CASES = {"pairing": case_pairing, "hops": case_hops, "eloc": case_eloc,
-         "proposal_sample": case_proposal_sample, "proposal_backward": case_proposal_backward}
+         "proposal_sample": case_proposal_sample, "proposal_backward": case_proposal_backward,
+         "resconv_tc": case_resconv_tc, "resconv": case_resconv}
 
 
 def main(argv=None):
