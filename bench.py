@@ -585,6 +585,72 @@ def measure_resconv(args, dev, st) -> dict:
     return out
 
 
+def measure_released_sampling(args, dev, st) -> dict:
+    """Sampling on a physical state: the released tpm02_L16_pfaffian (tensor-core residual
+    network) with the uniform hop and with the learned proposal trained on records drawn from the
+    released equilibrated chains (spins 1024..8191, ``released_repeats`` moves each, Barker
+    weight).  Both runs start from the stored chains 0..B-1 (already equilibrated under the
+    projected state) and measure ``released_steps`` steps: acceptance, tau_int of log|psi|,
+    effective samples/s and E/N on ``energy_samples`` final configurations."""
+    import torch
+
+    import neuralhubbard_b200 as nh
+    from neuralhubbard_b200 import checkpoint, stats
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    eqx = os.path.join(here, "tests", "golden", "released", "tpm02_L16_pfaffian.eqx")
+    if not os.path.exists(eqx):
+        return {"skipped": "released weights not fetched (tests/golden/fetch_released.py)"}
+    params = checkpoint.load_pfaffian_backflow(eqx, L)
+    spins = checkpoint.load_spins(eqx.replace(".eqx", "_spins.npz"), N_SITES)
+    info = checkpoint.RELEASED["tpm02_L16_pfaffian"]
+    ne = 7 * N_SITES // 16
+    state = nh.Variational(nh.PfaffianBackflow(L, L, ne, ne, params=params, cnn_mode=2,
+                                               device=dev), symm=True)
+    B, steps = args.chains, args.released_steps
+    pool = torch.from_numpy(spins[B:]).to(dev)
+    t0 = time.perf_counter()
+    psi_pool = state(pool)
+    recs = [nh.training_records(state, pool, psi=psi_pool, seed=900 + r, weight="barker")
+            for r in range(args.released_repeats)]
+    rec = tuple(torch.cat([r[i] for r in recs]) for i in range(len(recs[0])))
+    torch.cuda.synchronize()
+    t_rec = time.perf_counter() - t0
+    q = nh.HopProposal(L, L, 8, seed=901, std=0.05, device=dev)
+    t0 = time.perf_counter()
+    losses = q.train(rec, args.train_steps, batch=512, lr=3e-3, seed=902)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    out = {"state": "tpm02_L16_pfaffian (released), tensor-core residual network",
+           "chains": B, "measured_steps": steps,
+           "proposal_training": {"records": int(rec[0].shape[0]), "steps": args.train_steps,
+                                 "record_seconds": t_rec, "train_seconds": t_train,
+                                 "loss_first": float(np.mean(losses[:20])),
+                                 "loss_last": float(np.mean(losses[-20:]))}}
+    del rec, recs
+    H = nh.Hubbard(8.0, [1.0, info.tprime], [1, 2])
+    n_e = min(B, args.energy_samples)
+    start = torch.from_numpy(spins[:B]).to(dev)
+    for name, make in (("uniform_hop", lambda: nh.ParticleHop(state, B, n_neighbor=(1, 2),
+                                                              initial_spins=start, seed=903)),
+                       ("learned", lambda: nh.LearnedHop(state, B, q, initial_spins=start,
+                                                         seed=904))):
+        smp = make()
+        series, ms, acc = run_chains(smp, steps, st)
+        tau = stats.tau_int(series)
+        e = H.Oloc(state, nh.Samples(smp.spins[:n_e].contiguous(), smp.psi[:n_e]))
+        e = e.cpu().numpy() / N_SITES
+        out[name] = {"acceptance": acc, "tau_int_logpsi": tau, "ms_per_step": ms / steps,
+                     "effective_samples_per_s": stats.effective_rate(B, steps, tau, ms / 1e3),
+                     "energy_per_site": float(e.mean()),
+                     "energy_per_site_err": float(e.std(ddof=1) / np.sqrt(n_e))}
+        del smp
+    out["learned_vs_uniform"] = (out["learned"]["effective_samples_per_s"]
+                                 / out["uniform_hop"]["effective_samples_per_s"])
+    out["published_energy_per_site"] = info.energy
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -703,6 +769,9 @@ def run_ours(args) -> None:
     resconv = None
     if world == 1 and not args.no_resconv:
         resconv = measure_resconv(args, dev, st)
+    released_sampling = None
+    if world == 1 and args.released_sampling:
+        released_sampling = measure_released_sampling(args, dev, st)
 
     if rank == 0:
         cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
@@ -730,6 +799,7 @@ def run_ours(args) -> None:
             "large_lattice": large,
             "precision": precision,
             "resconv": resconv,
+            "released_sampling": released_sampling,
             "roofline": roof, "kernels": kernels, "gpu_launches": launches,
             "cpu_baseline": cpu, "clocks": clk,
         }
@@ -789,6 +859,10 @@ def main():
     ap.add_argument("--large-steps", type=int, default=2)
     ap.add_argument("--no-resconv", action="store_true",
                     help="skip the released-state residual network block")
+    ap.add_argument("--released-sampling", action="store_true",
+                    help="also compare uniform and learned hops on the released state")
+    ap.add_argument("--released-steps", type=int, default=1000)
+    ap.add_argument("--released-repeats", type=int, default=16)
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the precision-form report (errors against the all-FP64 path)")
     ap.add_argument("--chains", type=int, default=1024)
