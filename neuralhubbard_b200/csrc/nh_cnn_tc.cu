@@ -17,7 +17,8 @@
 // 32 (w % 4) .. + 31 of both tiles).
 //
 // Two warp groups of 128 threads run independent image streams in one CTA: each has its own
-// activation planes, bookkeeping, mbarrier, 64 tensor-memory columns and named barrier, and
+// activation planes, bookkeeping, mbarrier, 256 tensor-memory columns (four partial sums of its
+// two 128 x 32 tiles, see issue_layer) and named barrier, and
 // shares the resident weights; while one group's MMAs run, the other converts its accumulators
 // (bias, GELU, hi/lo split) and writes its next planes.
 //
@@ -52,7 +53,8 @@ constexpr int kActBytes = 2 * 4 * kPlane;        // hi and lo, 4 planes each
 constexpr int kWG = 2;                           // independent warp groups per CTA
 constexpr int kWGThreads = kTcThreads / kWG;     // 128
 constexpr int kIntsPerWG = 3 * 2 * kL * kL + 4 * kL + 32;  // simg, rowof, occl, scan scratch
-constexpr unsigned kTmemCols = 64 * kWG;         // two 128 x 32 FP32 accumulators per group
+constexpr int kParts = 4;                        // partial sums per tile: (kh, cross)
+constexpr unsigned kTmemCols = 64 * kParts * kWG; // per group: 4 partials x two 128 x 32 tiles
 
 struct TcArgs {
   ConfigList cl;
@@ -77,6 +79,10 @@ __device__ __forceinline__ float gelu_tanh(float x) {
 }
 
 // Issue the MMAs of one layer for both tiles (one thread).
+// Partial sum p = 2 kh + cross of tile h lives at columns 64 p + 32 h of the group's 256: the
+// hi*hi products of the input-channel half kh, and (cross = 1) its hi*lo + lo*hi products, so
+// that every FP32 accumulation chain in the tensor core is short (9 or 18 MMAs) and the small
+// cross terms are not added into the large main sum there.  The epilogue adds the partials.
 __device__ void issue_layer(uint32_t tmem, uint32_t act_hi, uint32_t act_lo, uint32_t w_hi,
                             uint32_t w_lo, int kchunks, int tap_bytes, bool split_act,
                             bool split_w) {
@@ -86,8 +92,6 @@ __device__ void issue_layer(uint32_t tmem, uint32_t act_hi, uint32_t act_lo, uin
   const uint32_t sbo_b = 128;      // next 8-co group of the weights
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    const uint32_t d = tmem + 32 * h;
-    bool acc = false;
 #pragma unroll
     for (int tap = 0; tap < 9; ++tap) {
       const int dx = tap / 3 - 1, dy = tap % 3 - 1;
@@ -95,16 +99,34 @@ __device__ void issue_layer(uint32_t tmem, uint32_t act_hi, uint32_t act_lo, uin
 #pragma unroll
       for (int kh = 0; kh < 2; ++kh) {
         if (kh >= kchunks / 2) break;
+        const uint32_t d_main = tmem + 64 * (2 * kh) + 32 * h;
+        const uint32_t d_cross = d_main + 64;
         const uint32_t ao = aoff + 2 * kh * kPlane;
         const uint32_t bo = tap * tap_bytes + 2 * kh * 4 * 128;
         const uint64_t ahi = make_desc(act_hi + ao, lbo_a, sbo_a);
         const uint64_t bhi = make_desc(w_hi + bo, lbo_b, sbo_b);
-        mma_bf16(d, ahi, bhi, kIdesc, acc);
-        acc = true;
-        if (split_w) mma_bf16(d, ahi, make_desc(w_lo + bo, lbo_b, sbo_b), kIdesc, true);
-        if (split_act) mma_bf16(d, make_desc(act_lo + ao, lbo_a, sbo_a), bhi, kIdesc, true);
+        mma_bf16(d_main, ahi, bhi, kIdesc, tap > 0);
+        if (split_w) mma_bf16(d_cross, ahi, make_desc(w_lo + bo, lbo_b, sbo_b), kIdesc, tap > 0);
+        if (split_act)
+          mma_bf16(d_cross, make_desc(act_lo + ao, lbo_a, sbo_a), bhi, kIdesc,
+                   tap > 0 || split_w);
       }
     }
+  }
+}
+
+// Accumulators of tile h for this warp's lane quarter: the sum of the partials the layer wrote.
+__device__ __forceinline__ void load_tile(uint32_t tlane, int h, int kchunks, bool cross,
+                                          float* v) {
+  tmem_ld32(tlane + 32 * h, v);
+#pragma unroll
+  for (int p = 1; p < kParts; ++p) {
+    const int kh = p >> 1;
+    if (kh >= kchunks / 2 || ((p & 1) && !cross)) continue;
+    float w[32];
+    tmem_ld32(tlane + 64 * p + 32 * h, w);
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] += w[i];
   }
 }
 
@@ -194,7 +216,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
   __syncthreads();
 
   // This warp group's state.
-  const uint32_t tmem = *tmem_slot + 64u * wg;
+  const uint32_t tmem = *tmem_slot + 64u * kParts * wg;
   unsigned char* act = act_all + wg * kActBytes;
   int* simg = ints_all + wg * kIntsPerWG;  // (2N) image configuration
   int* rowof = simg + M2;                  // (2N) mode -> row of Y, or -1
@@ -302,7 +324,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           float v[32];
-          tmem_ld32(tmem + ((uint32_t)(32 * lwid) << 16) + 32 * h, v);
+          load_tile(tmem + ((uint32_t)(32 * lwid) << 16), h, layer == 0 ? 2 : 4, split, v);
           act_groups(v, bl, hi[h], lo[h]);
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -320,7 +342,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           float v[32];
-          tmem_ld32(tmem + ((uint32_t)(32 * lwid) << 16) + 32 * h, v);
+          load_tile(tmem + ((uint32_t)(32 * lwid) << 16), h, 4, split, v);
           const int s = x * kL + 8 * h + (mrow & 7);
 #pragma unroll
           for (int sg = 0; sg < 2; ++sg) {
