@@ -157,3 +157,33 @@ def test_tau_int_matches_oracle_and_ar1():
     m0, err0 = osam.jackknife_mean(x[:, 0])
     assert m == m0 and abs(err - err0) < 1e-12
     assert stats.effective_rate(64, 4000, 0.5, 2.0) == 64 * 4000 / 2.0
+
+
+def test_residual_network_argument_checks():
+    """Packing sizes and the parameter checks of the residual network (net = NH_NET_RESCONV),
+    all decided before any device work."""
+    if not os.path.exists(LIB):
+        pytest.skip("libnh_b200.so not built")
+    from neuralhubbard_b200 import _lib
+
+    lib = _lib.load()
+    p8 = ctypes.c_void_p(4096)
+    assert lib.nh_pack_resconv_weights_floats(64, 16) == 4 * 64 + 32 * 9 * 64 * 64
+    assert lib.nh_pack_resconv_weights_tc_bytes(16) == 32 * 9 * 2 * 64 * 64 * 2
+    assert lib.nh_pack_resconv_weights(p8, 32, 16, p8, None) == -2
+    assert lib.nh_pack_resconv_weights(None, 64, 16, p8, None) == -1
+    assert lib.nh_pack_resconv_weights_tc(p8, 48, 16, p8, None) == -2
+
+    def amplitude(**kw):
+        f = dict(conv_w=4096, conv_b=4096, conv_w_packed=4096, conv_w_tc=4096, Wt=4096,
+                 Wt64=4096, Lx=16, Ly=16, n_up=112, n_dn=112, channels=64, layers=16,
+                 cnn_mode=0, pf_mode=0, net=_lib.NET_RESCONV, reserved=0, cond_tau=100.0,
+                 cancel_tau=8.0)
+        f.update(kw)
+        prm = _lib.BackflowParams(**f)
+        return lib.nh_amplitude(p8, 4, 8, ctypes.byref(prm), p8, p8, p8, p8, 1 << 30, None)
+
+    assert amplitude(channels=32) == -2 and b"64 channels" in lib.nh_last_error()
+    assert amplitude(cnn_mode=1) == -2
+    assert amplitude(cnn_mode=2, Lx=8, Ly=8, n_up=28, n_dn=28) == -2
+    assert amplitude(net=7) == -1 and b"net 7" in lib.nh_last_error()
