@@ -25,8 +25,8 @@ CUDA cores and on the tensor cores, with E/N of the released 16x16 state on 512 
 
 Under torchrun each rank evaluates its own 8192 configurations (weak scaling); the time is the
 maximum over ranks of the summed per-step CUDA-event durations.  ``--impl reference`` times the
-CPU restatement of the same path (the reference's JAX stack cannot be installed here) on all
-host cores, on rank 0 only.
+compiled CPU restatement of the same path (oracle/c/nh_port.c; the reference's JAX stack cannot
+be installed here) on all host cores, on rank 0 only.
 """
 
 from __future__ import annotations
@@ -138,15 +138,15 @@ def _cpu_worker(args):
 
 
 def cpu_baseline(target_s: float = 12.0) -> dict:
-    """Projected amplitudes of the same workload by the CPU restatement, all host cores in a
-    spawn pool (one numpy thread each), on a bounded sample sized for ~target_s seconds."""
+    """Projected amplitudes of the same workload by the CPU restatement on all host cores, on a
+    bounded sample sized for ~target_s seconds: the compiled restatement (oracle/c/nh_port.c,
+    gcc -O3, OpenMP across configurations) when it builds, else the numpy oracle in a spawn
+    pool (one numpy thread per core)."""
     import multiprocessing as mp
 
     from neuralhubbard_b200.backflow import init_params
     from neuralhubbard_b200.sampler import random_spins
 
-    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
-        os.environ[k] = "1"
     try:
         cores = len(os.sched_getaffinity(0))
     except Exception:
@@ -156,6 +156,30 @@ def cpu_baseline(target_s: float = 12.0) -> dict:
                   conv_b=[b.astype(np.float64) for b in p["conv_b"]],
                   W=p["W"].astype(np.float64), theta=float(p["theta"]), Lx=L, Ly=L)
     rng = np.random.default_rng(123)
+    try:
+        from oracle import port
+
+        port.load()
+    except Exception:
+        port = None
+    if port is not None:
+        warm = random_spins(rng, cores, N_SITES, NE, NE)
+        t0 = time.perf_counter()
+        port.projected_amplitude(warm, params, threads=cores)
+        t_batch = time.perf_counter() - t0
+        n_cfg = max(cores, int(cores * target_s / max(t_batch, 1e-3)))
+        sample = random_spins(rng, n_cfg, N_SITES, NE, NE)
+        t0 = time.perf_counter()
+        port.projected_amplitude(sample, params, threads=cores)
+        wall = time.perf_counter() - t0
+        n_amp = n_cfg * IMAGES
+        return {"value": n_amp / wall, "unit": UNIT, "cores": cores, "kind": "port",
+                "sample": f"{n_cfg} configurations x {IMAGES} images at 16x16 ({n_amp} "
+                          f"amplitudes, compiled FP64 restatement, gcc -O3 + OpenMP, "
+                          f"{wall:.1f} s)",
+                "seconds": wall}
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
         one = random_spins(rng, 1, N_SITES, NE, NE)
@@ -827,7 +851,8 @@ def run_reference(args) -> None:
         "data": "synthetic",
         "config": {"workload": "projected amplitudes, 16x16 Hubbard lattice, 112+112 electrons, "
                                "8 images per configuration (bounded sample per step)",
-                   "form": "CPU restatement of the reference path (JAX stack not installable)",
+                   "form": "compiled CPU restatement of the reference path (C, FP64, OpenMP "
+                           "across configurations; the JAX stack is not installable)",
                    "L": L, "images": IMAGES},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": last["cores"], "kind": "port",
                          "sample": last["sample"]},

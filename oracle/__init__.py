@@ -27,13 +27,19 @@ What it restates (reference paths relative to the ChenAo-Phys/NeuralHubbard tree
                   step, integrated autocorrelation time, block jackknife
                   (``code/measure/assemble.py:48-84``).
 * ``proposal``    the learned hop-proposal CNN forward/backward (FP64), for gradient checks.
+* ``resconv``     the released states' residual network (16 blocks x 64 channels,
+                  ``code/backflow/models.py:319-329``), restated from its published description.
+* ``port``        ctypes wrapper of ``c/nh_port.c``, the same projected amplitude compiled
+                  (gcc, OpenMP): the CPU baseline of ``bench.py``, checked against the numpy code.
 
 Parity status: the Pfaffian is pinned by known-answer tests from mathematics
 (pf^2 = det, pf(B^T A B) = det(B) pf(A), block-diagonal products, brute-force expansion);
 the Hamiltonian by a Fock-space brute force; the gather by its two reference formulas
 (kernel order and einsum twin) agreeing.  The conventions that live inside quantax 0.4.0
 and fermix 0.1.0 (``fermion_inverse_sign``, the exact Flip maps and image signs, the
-projection normalisation) cannot be executed here (no JAX in this image), so for those the
-parity is unpinned: they are defined from the mathematics of the second-quantised state and
-documented in ``projection`` and ``hubbard``.
+projection normalisation, the residual network) cannot be executed here (no JAX in this
+image); they are defined from the mathematics of the second-quantised state and the
+published network description, and pinned together end to end by the released
+``tpm02_L16_pfaffian`` state: its projected local energy on its own stored chains reproduces
+the published E/N (``tests/test_gpu_resconv.py``).
 """
