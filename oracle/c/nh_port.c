@@ -73,31 +73,42 @@ static int cnn(const Net* net, Work* w, const int8_t* s) {
   int cin = 2;
   for (int l = 0; l < net->layers; ++l) {
     const double* bl = net->conv_b + (size_t)l * C;
-    for (int o = 0; o < C; ++o) {
-      double* po = out + o * plane;
-      for (int x = 0; x < Lx; ++x)
-        for (int y = 0; y < Ly; ++y) po[(x + 1) * P + y + 1] = bl[o];
-      for (int i = 0; i < cin; ++i) {
-        const double* pi = in + i * plane;
-        const double* wk = wl + ((size_t)o * cin + i) * 9;
-        for (int u = 0; u < 3; ++u)
-          for (int v = 0; v < 3; ++v) {
-            const double wv = wk[u * 3 + v];
-            for (int x = 0; x < Lx; ++x) {
-              double* dst = po + (x + 1) * P + 1;
-              const double* src = pi + (x + u) * P + v;
-              for (int y = 0; y < Ly; ++y) dst[y] += wv * src[y];
+    /* Four output channels at a time: each input row is loaded once for four FMA streams. */
+    for (int o0 = 0; o0 < C; o0 += 4) {
+      const int no = C - o0 < 4 ? C - o0 : 4;
+      for (int x = 0; x < Lx; ++x) {
+        double acc[4][64];
+        for (int j = 0; j < no; ++j)
+          for (int y = 0; y < Ly; ++y) acc[j][y] = bl[o0 + j];
+        for (int i = 0; i < cin; ++i) {
+          const double* pi = in + i * plane;
+          for (int u = 0; u < 3; ++u) {
+            const double* srow = pi + (x + u) * P;
+            for (int v = 0; v < 3; ++v) {
+              const double* src = srow + v;
+              double wv[4];
+              for (int j = 0; j < 4; ++j)
+                wv[j] = j < no ? wl[((size_t)(o0 + j) * cin + i) * 9 + u * 3 + v] : 0.0;
+              for (int y = 0; y < Ly; ++y) {
+                const double sv = src[y];
+                acc[0][y] += wv[0] * sv;
+                acc[1][y] += wv[1] * sv;
+                acc[2][y] += wv[2] * sv;
+                acc[3][y] += wv[3] * sv;
+              }
             }
           }
-      }
-      if (l < net->layers - 1) {
-        for (int x = 0; x < Lx; ++x) {
-          double* q = po + (x + 1) * P + 1;
-          for (int y = 0; y < Ly; ++y) q[y] = gelu_tanh(q[y]);
+        }
+        for (int j = 0; j < no; ++j) {
+          double* dst = out + (o0 + j) * plane + (x + 1) * P + 1;
+          if (l < net->layers - 1)
+            for (int y = 0; y < Ly; ++y) dst[y] = gelu_tanh(acc[j][y]);
+          else
+            for (int y = 0; y < Ly; ++y) dst[y] = acc[j][y];
         }
       }
-      fill_halo(po, Lx, Ly);
     }
+    for (int o = 0; o < C; ++o) fill_halo(out + o * plane, Lx, Ly);
     wl += (size_t)C * cin * 9;
     cin = C;
     double* t = in;
@@ -221,8 +232,8 @@ int nhp_amplitudes(const int8_t* spins, int B, int Lx, int Ly, int C, int layers
                    const double* conv_w, const double* conv_b, const double* Wt, int n,
                    const int64_t* maps, int G, double* sign, double* logabs, int nthreads) {
   if (!spins || !conv_w || !conv_b || !Wt || !maps || !sign || !logabs || B < 0 || G < 1 ||
-      C < 2 || C % 2 || layers < 1 || n < 2)
-    return -1;
+      C < 2 || C % 2 || layers < 1 || n < 2 || Ly > 64 || G > 64)
+    return -1; /* (the row accumulators hold 64 sites, the image sums 64 images) */
   Net net = {Lx, Ly, Lx * Ly, C, layers, C / 2, n, G, conv_w, conv_b, Wt, maps};
   const int N = net.N;
   int err = 0;
