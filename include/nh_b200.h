@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define NH_ABI_VERSION 6
+#define NH_ABI_VERSION 7
 
 enum {
   NH_OK = 0,
@@ -46,8 +46,10 @@ enum {
   NH_FLAG_ZERO_PIVOT = 1,  /* exactly singular pairing block: sign 0, logabs -inf */
   NH_FLAG_NONFINITE = 2,   /* a non-finite value met during the factorisation */
   NH_FLAG_GROWTH = 4,      /* pivot ratio above cond_tau (near-nodal, ill-conditioned block) */
-  NH_FLAG_REFINED = 8,     /* recomputed in FP64 because of NH_FLAG_GROWTH */
-  NH_FLAG_CANCEL = 16      /* projected amplitude: sum_g |psi_g| > cancel_tau |sum_g eta_g psi_g| */
+  NH_FLAG_REFINED = 8,     /* log-Pfaffian refined in FP64 (see refine_tau and cond_tau) */
+  NH_FLAG_CANCEL = 16,     /* projected amplitude: sum_g |psi_g| > cancel_tau |sum_g eta_g psi_g| */
+  NH_FLAG_TIMEOUT = 32     /* a bounded wait of a tensor-core kernel expired during this call:
+                              the amplitudes it aborted are NaN; treat the whole call as failed */
 };
 
 /* Backflow networks (nh_backflow_params.net). */
@@ -80,12 +82,19 @@ enum {
  * Wt:            FP32 (4, N, d) spin-block table from nh_build_wtilde, blocks [uu, ud, du, dd].
  * Wt64:          the same table in FP64 (nh_build_wtilde), or null to disable the FP64
  *                recompute of ill-conditioned items.
- * cond_tau:      an item whose largest / smallest pivot magnitude exceeds cond_tau is flagged
- *                NH_FLAG_GROWTH and, when Wt64 is set, recomputed end to end in FP64
- *                (CNN, gather, Pfaffian; NH_FLAG_REFINED); <= 0 disables both.  For projected
- *                amplitudes with cond_tau > 1 an image whose |psi(g s)| is below 1e-3 of
- *                |psi_P(s)| is not recomputed (its error cannot move log|psi_P| by more than
- *                ~1e-5); cond_tau <= 1 recomputes every image (the all-FP64 form).
+ * refine_tau:    an item whose largest / smallest FP32 pivot magnitude exceeds refine_tau has its
+ *                log-Pfaffian refined: the same matrix is factorised again in FP64 with the
+ *                pivot order of the FP32 factorisation held fixed (no pivot search; a blocked
+ *                rank-8 FP64 elimination), which removes the FP32 factorisation error
+ *                (NH_FLAG_REFINED).  <= 0: off; 1: every item.  Needs n <= 224; for larger n the
+ *                refinement is the pivoted FP64 recompute of cond_tau below.
+ * cond_tau:      an item whose pivot ratio exceeds cond_tau is flagged NH_FLAG_GROWTH and, when
+ *                Wt64 is set, its features are recomputed in FP64 (CNN) and its log-Pfaffian is
+ *                refined against the FP64 pairing block (NH_FLAG_REFINED; n > 224: a pivoted
+ *                FP64 Pfaffian); <= 0 disables both.  For projected amplitudes with
+ *                cond_tau > 1 an image whose |psi(g s)| is below 1e-3 of |psi_P(s)| is not
+ *                recomputed in FP64 (its error cannot move log|psi_P| by more than ~1e-5);
+ *                cond_tau <= 1 recomputes every image (the all-FP64 form).
  * cancel_tau:    projected amplitudes only: a configuration whose 8 images cancel, i.e.
  *                sum_g |psi(g s)| > cancel_tau |sum_g eta_g psi(g s)|, amplifies the FP32
  *                error of its images by that factor; with cancel_tau > 0 (and Wt64 set) all its
@@ -108,6 +117,7 @@ typedef struct {
   int32_t reserved;
   double cond_tau;
   double cancel_tau;
+  double refine_tau;
 } nh_backflow_params;
 
 /* Hubbard model H = -sum t_ij c+_i c_j + U sum n_up n_dn; n_dirs = 4 (nearest) or 8
@@ -151,6 +161,7 @@ enum {
   NH_K_RESCONV = 22,
   NH_K_RESCONV64 = 23,
   NH_K_RESCONV_TC = 24,
+  NH_K_REFINE = 25,
   NH_K_COUNT = 32
 };
 int nh_profile_enable(int on);
@@ -194,10 +205,11 @@ int nh_pairing_occ(const float* Y, const int32_t* idx, const float* Wt, int Lx, 
 
 /* sign and log|pf| of batch antisymmetric n x n FP32 matrices (n even, n <= 1024); only the
  * strict lower triangle is read.  With cond_tau > 0 the matrices whose pivot ratio exceeds it
- * are flagged NH_FLAG_GROWTH and factorised again in FP64 (NH_FLAG_REFINED).  The workspace
- * (nh_slogpf_workspace_bytes(n, batch) bytes) holds the list of those matrices and, where a
- * triangle exceeds shared memory (FP32 n > 256, FP64 n > 236), one triangle per SM; it may be
- * null when cond_tau <= 0 and n <= 256. */
+ * are flagged NH_FLAG_GROWTH and factorised again in FP64 (NH_FLAG_REFINED): for n <= 224 with
+ * the pivot order of the FP32 factorisation held fixed, beyond with FP64 partial pivoting.  The
+ * workspace (nh_slogpf_workspace_bytes(n, batch) bytes) holds the list of those matrices, their
+ * FP32 pivot orders and, where a triangle exceeds shared memory (FP32 n > 256, FP64 n > 236), one
+ * triangle per SM; it may be null when cond_tau <= 0 and n <= 256. */
 size_t nh_slogpf_workspace_bytes(int n, int batch);
 int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, double* logabs,
               int32_t* flags, void* workspace, size_t workspace_bytes, void* stream);

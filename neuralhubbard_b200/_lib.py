@@ -16,6 +16,8 @@ LIB_PATH = os.path.join(_HERE, "libnh_b200.so")
 NH_OK = 0
 NET_CNN, NET_RESCONV = 0, 1
 FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH, FLAG_REFINED, FLAG_CANCEL = 1, 2, 4, 8, 16
+FLAG_TIMEOUT = 32
+ABI_VERSION = 7
 
 c_void_p, c_int, c_int64, c_uint64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64
 c_float, c_double, c_size_t = ctypes.c_float, ctypes.c_double, ctypes.c_size_t
@@ -45,6 +47,7 @@ class BackflowParams(ctypes.Structure):
         ("reserved", ctypes.c_int32),
         ("cond_tau", c_double),
         ("cancel_tau", c_double),
+        ("refine_tau", c_double),
     ]
 
 
@@ -133,8 +136,32 @@ def load() -> ctypes.CDLL:
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
+        if lib.nh_abi_version() != ABI_VERSION:
+            raise NativeLibraryError(f"{LIB_PATH} has ABI {lib.nh_abi_version()}, this package "
+                                     f"expects {ABI_VERSION}; rebuild it")
         _lib = lib
         return lib
+
+
+class DeviceTimeoutError(NativeLibraryError):
+    """A bounded wait of a tensor-core kernel expired: the call's results are not valid."""
+
+
+def timeout_flagged(flags) -> bool:
+    """Whether any of the output flags (numpy array or torch tensor) carries FLAG_TIMEOUT."""
+    if hasattr(flags, "cpu"):
+        flags = flags.cpu().numpy()
+    import numpy as np
+
+    return bool((np.asarray(flags) & FLAG_TIMEOUT).any())
+
+
+def check_flags(flags, what: str) -> None:
+    """Raise DeviceTimeoutError when an output flag carries FLAG_TIMEOUT (the tensor-core
+    kernels' device error word, folded into the flags by the image combination)."""
+    if flags is not None and timeout_flagged(flags):
+        raise DeviceTimeoutError(f"{what}: a tensor-core kernel's bounded wait expired "
+                                 "(NH_FLAG_TIMEOUT); its amplitudes are NaN")
 
 
 def check(rc: int, what: str) -> None:
@@ -148,7 +175,7 @@ KERNEL_IDS = {
     "hop_emit": 6, "eloc_reduce": 7, "mh_propose": 8, "compact": 9, "mh_accept": 10,
     "wtilde": 11, "pfaffian64": 12, "cnn64": 13, "flagged": 14, "pack": 15, "cnn_tc": 16,
     "pfaffian_tc": 17, "prop_sample": 18, "prop_forward": 19, "prop_backward": 20,
-    "prop_adam": 21, "resconv": 22, "resconv64": 23, "resconv_tc": 24,
+    "prop_adam": 21, "resconv": 22, "resconv64": 23, "resconv_tc": 24, "refine": 25,
 }
 K_COUNT = 32
 

@@ -121,13 +121,18 @@ DEFAULT_COND_TAU = 100.0
 # Projected amplitudes whose 8 images cancel by more than this factor are recomputed in FP64:
 # the cancellation amplifies the FP32 error of the images by the same factor.
 DEFAULT_CANCEL_TAU = 8.0
+# Images whose FP32 pivot ratio exceeds this are refined in FP64 with their FP32 pivot order
+# (a blocked static-pivot elimination, no pivot search): it removes the FP32 factorisation
+# error, the dominant error of an FP32 log-Pfaffian at n = 224.
+DEFAULT_REFINE_TAU = 10.0
 
 
 def slogpf(F: torch.Tensor, cond_tau: float = DEFAULT_COND_TAU):
     """(sign FP32, logabs FP64, flags int32) of the Pfaffians of antisymmetric F (..., n, n)
     in FP32, n even and at most 1024; only the strict lower triangle is read.  Matrices whose
     pivot ratio exceeds ``cond_tau`` are factorised again in FP64 (flags NH_FLAG_GROWTH |
-    NH_FLAG_REFINED); ``cond_tau=0`` keeps the plain FP32 result."""
+    NH_FLAG_REFINED): for n <= 224 with the pivot order of the FP32 factorisation held fixed,
+    beyond with FP64 partial pivoting; ``cond_tau=0`` keeps the plain FP32 result."""
     F = _require_cuda(F, torch.float32, "F")
     n = F.shape[-1]
     if F.shape[-2] != n:
@@ -154,15 +159,19 @@ class PfaffianBackflow:
     def __init__(self, Lx: int, Ly: int, n_up: int, n_dn: int, params: Optional[dict] = None,
                  channels: int = 32, layers: int = 4, seed: int = 0, device="cuda",
                  cond_tau: float = DEFAULT_COND_TAU, cnn_mode: int = 0,
-                 pf_mode: int = 0, cancel_tau: float = DEFAULT_CANCEL_TAU):
+                 pf_mode: int = 0, cancel_tau: float = DEFAULT_CANCEL_TAU,
+                 refine_tau: float = DEFAULT_REFINE_TAU):
         """``cond_tau``: items whose pivot ratio exceeds it are recomputed end to end in FP64
         (``0`` keeps every item on the FP32 path).  ``cnn_mode``: 0 FP32 CUDA cores, 1 tcgen05
         BF16, 2 tcgen05 BF16 x3 (near-FP32); modes 1 and 2 need 16x16, 32 channels, 4 layers.
         ``pf_mode``: 0 Pfaffian on CUDA cores, 1 matrix in tensor memory with tcgen05 updates.
         ``cancel_tau`` (projected amplitudes): configurations whose images cancel by more than
-        this factor are recomputed in FP64 (0 = off; default 8)."""
+        this factor are recomputed in FP64 (0 = off; default 8).  ``refine_tau``: images whose
+        FP32 pivot ratio exceeds it get their log-Pfaffian refined in FP64 with the FP32 pivot
+        order (0 = off, 1 = every image; n <= 224)."""
         self.device = torch.device(device)
         self.cond_tau = float(cond_tau)
+        self.refine_tau = float(refine_tau)
         self.cnn_mode = int(cnn_mode)
         self.pf_mode = int(pf_mode)
         self.cancel_tau = float(cancel_tau)
@@ -214,7 +223,7 @@ class PfaffianBackflow:
                                    self.conv_w_packed.data_ptr(), _ptr(self.conv_w_tc),
                                    self.Wt.data_ptr(), self.Wt64.data_ptr(), g.LX, g.LY, g.n_up,
                                    g.n_dn, self.channels, self.layers, self.cnn_mode, self.pf_mode,
-                                   self.net, 0, self.cond_tau, self.cancel_tau)
+                                   self.net, 0, self.cond_tau, self.cancel_tau, self.refine_tau)
 
     def features(self, spins: torch.Tensor) -> torch.Tensor:
         """(B, 2, N, d) backflow features of int8 configurations (B, 2N)."""

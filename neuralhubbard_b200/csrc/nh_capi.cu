@@ -99,6 +99,13 @@ static size_t act_scratch_bytes(const nh_backflow_params& p) {
   return p.net == NH_NET_RESCONV ? resconv_scratch_bytes(N) : cnn_scratch_bytes(N, p.channels);
 }
 
+// Pivot-order records and refinement scratch: only where the FP64 refinement applies.
+static size_t refine_bytes(size_t items, int n) {
+  if (n > kRefineMaxN) return 0;
+  return align256(items * perm_stride(n) * sizeof(uint16_t)) + align256(items * sizeof(int32_t)) +
+         align256(sizeof(int32_t)) + align256(refine_slice_bytes(n));
+}
+
 size_t pipeline_bytes(int max_items, const nh_backflow_params& p) {
   const size_t it = (size_t)(max_items > 0 ? max_items : 1);
   const size_t n = (size_t)(p.n_up + p.n_dn), d = (size_t)(p.channels / 2);
@@ -107,7 +114,7 @@ size_t pipeline_bytes(int max_items, const nh_backflow_params& p) {
          align256(it * sizeof(int32_t)) * 2 + align256(sizeof(int32_t)) +
          align256(it * n * d * sizeof(double)) + align256(it * n * sizeof(int32_t)) +
          align256(sizeof(int32_t)) + align256(pfaffian_scratch_bytes((int)n)) +
-         align256(act_scratch_bytes(p));
+         align256(act_scratch_bytes(p)) + refine_bytes(it, (int)n);
 }
 
 PipelineBuffers carve_pipeline(void* ws, int max_items, const nh_backflow_params& prm) {
@@ -134,20 +141,32 @@ PipelineBuffers carve_pipeline(void* ws, int max_items, const nh_backflow_params
   const size_t tri_bytes = pfaffian_scratch_bytes((int)n), act_bytes = act_scratch_bytes(prm);
   b.pf_tri = tri_bytes ? take(tri_bytes) : nullptr;
   b.cnn_act = act_bytes ? take(act_bytes) : nullptr;
+  b.perm = nullptr;
+  b.list32 = b.count32 = nullptr;
+  b.slice = nullptr;
+  if ((int)n <= kRefineMaxN) {
+    b.perm = reinterpret_cast<uint16_t*>(take(it * perm_stride((int)n) * sizeof(uint16_t)));
+    b.list32 = reinterpret_cast<int32_t*>(take(it * sizeof(int32_t)));
+    b.count32 = reinterpret_cast<int32_t*>(take(sizeof(int32_t)));
+    b.slice = take(refine_slice_bytes((int)n));
+  }
   return b;
 }
 
-// CNN -> gather + Pfaffian (FP32) -> FP64 recompute of the items flagged ill-conditioned ->
-// combination of the symmetry images (or a copy for G = 1).
+// CNN -> gather + Pfaffian (FP32, recording each item's pivot order) -> FP64 features for the
+// items flagged ill-conditioned or cancelling -> FP64 refinement of the log-Pfaffian with the
+// FP32 pivot order (against the FP64 pairing block for those items, against the item's own FP32
+// block for the others above refine_tau) -> combination of the symmetry images (or a copy for
+// G = 1).  Beyond n = kRefineMaxN the flagged items are recomputed by the pivoted FP64 kernel.
 int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const PipelineBuffers& b,
                  float* sign, double* logabs, int32_t* flags, cudaStream_t st) {
   const int n = p.n_up + p.n_dn, d = p.channels / 2;
   const int max_items = cl.n_cfg * cl.G;
   if (max_items <= 0) return NH_OK;
   int rc;
-  if (p.cnn_mode == 1 || p.cnn_mode == 2 || p.pf_mode == 1)
-    if ((rc = check_cuda(cudaMemsetAsync(b.err, 0, sizeof(int32_t), st), "clear error word")))
-      return rc;
+  const bool tc = p.cnn_mode == 1 || p.cnn_mode == 2 || p.pf_mode == 1;
+  if (tc && (rc = check_cuda(cudaMemsetAsync(b.err, 0, sizeof(int32_t), st), "clear error word")))
+    return rc;
   if (p.net == NH_NET_RESCONV && p.cnn_mode == 2) {
     rc = launch_resconv_tc(cl, p, b.Y, b.idx, b.item_sign, b.err, st);
   } else if (p.cnn_mode == 1 || p.cnn_mode == 2) {
@@ -158,12 +177,18 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
     rc = launch_cnn(c, st);
   }
   if (rc) return rc;
+  const bool refine = b.perm != nullptr;  // n <= kRefineMaxN
   PfGatherArgs g{b.Y, b.idx, p.Wt, p.Lx, p.Ly, d, n, cl.n_cfg_dev, cl.G, max_items, nullptr,
                  b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, p.cond_tau, 0, false, b.pf_tri};
+  if (refine) {
+    g.perm = b.perm;
+    g.refine_tau = p.refine_tau;
+  }
   if ((rc = p.pf_mode == 1 ? launch_pfaffian_tc(g, 1, nullptr, b.err, st)
                            : launch_pfaffian_gather(g, st)))
     return rc;
-  if (p.Wt64 && (p.cond_tau > 0.0 || (p.cancel_tau > 0.0 && cl.G > 1))) {
+  const bool fp64 = p.Wt64 && (p.cond_tau > 0.0 || (p.cancel_tau > 0.0 && cl.G > 1));
+  if (fp64) {
     // cond_tau <= 1 flags every image (the all-FP64 form): nothing is pruned then.
     if ((rc = launch_image_mark(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev,
                                 p.cancel_tau, p.cond_tau > 1.0, st)))
@@ -173,13 +198,31 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
     CnnLaunch c64{&cl, &p, 1, true, b.list, b.count, max_items, nullptr, b.Y64, b.idx64,
                   b.item_sign, b.cnn_act};
     if ((rc = launch_cnn(c64, st))) return rc;
-    PfGatherArgs g64{b.Y64, b.idx64, p.Wt64, p.Lx, p.Ly, d, n, b.count, 1, max_items, b.list,
-                     b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, 0.0,
-                     NH_FLAG_GROWTH | NH_FLAG_REFINED, true, b.pf_tri};
-    if ((rc = launch_pfaffian_gather(g64, st))) return rc;
+    if (refine) {
+      RefineLaunch r{n, d, 2, nullptr, b.Y64, b.idx64, p.Wt64, p.Lx, p.Ly, b.list, b.count,
+                     max_items, b.perm, perm_stride(n), b.item_sign, b.pf_sign, b.pf_logabs,
+                     b.pf_flags, b.slice};
+      if ((rc = launch_refine(r, st))) return rc;
+    } else {
+      PfGatherArgs g64{b.Y64, b.idx64, p.Wt64, p.Lx, p.Ly, d, n, b.count, 1, max_items, b.list,
+                       b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, 0.0,
+                       NH_FLAG_GROWTH | NH_FLAG_REFINED, true, b.pf_tri};
+      if ((rc = launch_pfaffian_gather(g64, st))) return rc;
+    }
+  }
+  if (refine && p.refine_tau > 0.0) {
+    // Items above refine_tau that did not get FP64 features: refined against their FP32 block.
+    const int skip = NH_FLAG_ZERO_PIVOT | NH_FLAG_REFINED;
+    if ((rc = launch_flagged(b.pf_flags, max_items, cl.n_cfg_dev, cl.G, b.list32, b.count32, st,
+                             kFlagNeedRefine, skip)))
+      return rc;
+    RefineLaunch r{n, d, 1, nullptr, b.Y, b.idx, p.Wt, p.Lx, p.Ly, b.list32, b.count32, max_items,
+                   b.perm, perm_stride(n), b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags,
+                   b.slice};
+    if ((rc = launch_refine(r, st))) return rc;
   }
   return launch_combine(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev, sign,
-                        logabs, flags, p.cancel_tau, st);
+                        logabs, flags, p.cancel_tau, tc ? b.err : nullptr, st);
 }
 
 static int check_params(const nh_backflow_params* p) {
@@ -332,11 +375,17 @@ int nh_pairing_occ(const float* Y, const int32_t* idx, const float* Wt, int Lx, 
   return launch_pairing(Y, idx, Wt, Lx, Ly, d, n, batch, F, static_cast<cudaStream_t>(stream));
 }
 
-// Layout: [per-CTA triangles when n exceeds shared memory][refinement list (batch)][count].
+// Layout: [per-CTA triangles when n exceeds shared memory][refinement list (batch)][count]
+// [pivot orders (batch) and the refinement's per-CTA slice, n <= kRefineMaxN].
 size_t nh_slogpf_workspace_bytes(int n, int batch) {
-  const size_t tri = (n > 0 && n % 2 == 0 && n <= kMaxN) ? align256(pfaffian_scratch_bytes(n)) : 0;
-  return tri + align256((size_t)(batch > 0 ? batch : 1) * sizeof(int32_t)) +
-         align256(sizeof(int32_t));
+  const bool ok = n > 0 && n % 2 == 0 && n <= kMaxN;
+  const size_t tri = ok ? align256(pfaffian_scratch_bytes(n)) : 0;
+  const size_t b = (size_t)(batch > 0 ? batch : 1);
+  const size_t ref = (ok && n <= kRefineMaxN)
+                         ? align256(b * perm_stride(n) * sizeof(uint16_t)) +
+                               align256(refine_slice_bytes(n))
+                         : 0;
+  return tri + align256(b * sizeof(int32_t)) + align256(sizeof(int32_t)) + ref;
 }
 
 int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, double* logabs,
@@ -348,7 +397,8 @@ int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, do
   if (refine && !flags) return fail(NH_ERR_INVALID, "slogpf: refinement needs flags");
   if (batch == 0) return NH_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  // Scratch: the FP64 triangles when refining, the FP32 ones beyond n = 256.
+  // Scratch: the refinement list (and, n <= kRefineMaxN, the pivot orders) when refining, the
+  // FP32 triangles beyond n = 256, the FP64 ones beyond 236.
   const bool scratch = pfaffian_needs_scratch(n, refine);
   int rc;
   if ((refine || scratch) &&
@@ -357,13 +407,24 @@ int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, do
     return rc;
   const size_t tri_bytes = align256(pfaffian_scratch_bytes(n));
   void* tri = tri_bytes ? workspace : nullptr;
-  rc = launch_pfaffian_from_F(F, n, batch, nullptr, nullptr, false, cond_tau, 0, sign, logabs,
-                              flags, tri, st);
-  if (rc || !refine) return rc;
   char* w = static_cast<char*>(workspace) + tri_bytes;
-  int32_t* list = reinterpret_cast<int32_t*>(w);
-  int32_t* count = reinterpret_cast<int32_t*>(w + align256((size_t)batch * sizeof(int32_t)));
+  int32_t* list = refine ? reinterpret_cast<int32_t*>(w) : nullptr;
+  w += align256((size_t)batch * sizeof(int32_t));
+  int32_t* count = refine ? reinterpret_cast<int32_t*>(w) : nullptr;
+  w += align256(sizeof(int32_t));
+  const bool static_pivot = refine && n <= kRefineMaxN;
+  uint16_t* perm = static_pivot ? reinterpret_cast<uint16_t*>(w) : nullptr;
+  void* slice = static_pivot ? w + align256((size_t)batch * perm_stride(n) * sizeof(uint16_t))
+                             : nullptr;
+  rc = launch_pfaffian_from_F(F, n, batch, nullptr, nullptr, false, cond_tau, 0, sign, logabs,
+                              flags, tri, st, perm, 0.0);
+  if (rc || !refine) return rc;
   if ((rc = launch_flagged(flags, batch, nullptr, 1, list, count, st))) return rc;
+  if (static_pivot) {
+    RefineLaunch r{n, 16, 0, F, nullptr, nullptr, nullptr, 0, 0, list, count, batch, perm,
+                   perm_stride(n), nullptr, sign, logabs, flags, slice};
+    return launch_refine(r, st);
+  }
   return launch_pfaffian_from_F(F, n, batch, list, count, true, 0.0,
                                 NH_FLAG_GROWTH | NH_FLAG_REFINED, sign, logabs, flags, tri, st);
 }

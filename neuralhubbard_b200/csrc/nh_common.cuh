@@ -11,6 +11,16 @@ namespace nh {
 constexpr int kNumThreads = 256;  // block size of every per-item kernel
 constexpr int kMaxN = 1024;       // sites per lattice supported by the bookkeeping kernels
 
+// Internal per-item flag (never returned to callers; cleared by the refinement and masked by the
+// image combination): the FP32 pivot ratio exceeds refine_tau, so the item's log-Pfaffian is
+// refined in FP64 with its FP32 pivot order.
+constexpr int kFlagNeedRefine = 1 << 20;
+constexpr int kPublicFlags = 0xFFFF;
+// FP64 refinement with the FP32 pivot order (nh_refine.cu): its FP64 triangle lives in shared
+// memory, so n <= kRefineMaxN; beyond, flagged items are recomputed by the pivoted FP64 kernel.
+constexpr int kRefineMaxN = 224;
+constexpr size_t kRefineSmemLimit = 225 * 1024;
+
 // ------------------------------------------------------------------ host-side error state
 void set_error(const char* fmt, ...);
 int fail(int code, const char* fmt, ...);
@@ -220,7 +230,38 @@ struct PipelineBuffers {
   int32_t* err;       // (1,) device error word of the tensor-core CNN
   void* pf_tri;       // large lattices: per-CTA Pfaffian triangles (pfaffian_scratch_bytes)
   void* cnn_act;      // large lattices: per-CTA CNN activation planes (cnn_scratch_bytes)
+  uint16_t* perm;     // (items, perm_stride) FP32 pivot order of every item (n <= kRefineMaxN)
+  int32_t* list32;    // (items,) items refined against their FP32 matrix
+  int32_t* count32;   // (1,) their number
+  void* slice;        // refinement: per-CTA permuted triangles (refine_slice_bytes)
 };
+
+// uint16 words per item of the pivot-order record: perm[0, n) then the relabelling parity.
+__host__ __device__ __forceinline__ int perm_stride(int n) { return (n + 1 + 7) & ~7; }
+
+// FP64 refinement of items listed in list[0, *count) (nh_refine.cu).
+struct RefineLaunch {
+  int n, d;
+  int mode;  // 0: dense FP32 F (items, n, n); 1: gather FP32 Y / idx (indexed by item);
+             // 2: gather FP64 Y64 / idx64 (indexed by slot) with Wt64
+  const float* F;
+  const void* Y;
+  const int32_t* idx;
+  const void* Wt;
+  int Lx, Ly;
+  const int32_t* list;
+  const int32_t* count;
+  int max_slots;  // host upper bound of *count
+  const uint16_t* perm;
+  int perm_stride;
+  const float* item_sign;
+  float* sign;
+  double* logabs;
+  int32_t* flags;
+  void* slice;  // refine_slice_bytes(n), required by the gather modes
+};
+int launch_refine(const RefineLaunch& q, cudaStream_t st);
+size_t refine_slice_bytes(int n);
 
 size_t pipeline_bytes(int max_items, const nh_backflow_params& p);
 PipelineBuffers carve_pipeline(void* ws, int max_items, const nh_backflow_params& p);
@@ -258,6 +299,8 @@ struct PfGatherArgs {
   int flag_or;
   bool fp64;
   void* tri;  // per-CTA triangles for n beyond shared memory (pfaffian_scratch_bytes), or null
+  uint16_t* perm = nullptr;  // when set: the pivot order of every item (perm_stride(n) words)
+  double refine_tau = 0.0;   // pivot ratio above which kFlagNeedRefine is set (0: never)
 };
 
 // Launchers (return NH_OK or an error code).
@@ -268,7 +311,7 @@ int launch_pack_cnn(const float* conv_w, int channels, int layers, float* packed
 int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list,
                            const int32_t* count, bool fp64, double cond_tau, int flag_or,
                            float* sign, double* logabs, int32_t* flags, void* tri,
-                           cudaStream_t st);
+                           cudaStream_t st, uint16_t* perm = nullptr, double refine_tau = 0.0);
 int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st);
 // Tensor-memory Pfaffian (one matrix per SM, trailing updates on tcgen05): mode 1 gathers from
 // g.Y / g.idx / g.Wt (FP32), mode 0 reads dense F (items, n, n) FP32.
@@ -276,16 +319,20 @@ int launch_pfaffian_tc(const PfGatherArgs& g, int mode, const float* F, int32_t*
                        cudaStream_t st);
 int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,
                    int n, int batch, float* F, cudaStream_t st);
+// err (or null): the device error word of the tensor-core kernels; when it is set every
+// output flag carries NH_FLAG_TIMEOUT.
 int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, int n_cfg,
                    const int32_t* n_cfg_dev, float* sign, double* logabs, int32_t* flags,
-                   double cancel_tau, cudaStream_t st);
+                   double cancel_tau, const int32_t* err, cudaStream_t st);
 // Projected amplitudes (G > 1): marks every image of a configuration whose images cancel
 // (sum |.| > cancel_tau |sum|) with NH_FLAG_GROWTH | NH_FLAG_CANCEL, and unmarks ill-conditioned
 // images too small to matter, before the FP64 recompute list is built.
 int launch_image_mark(const float* sg, const double* la, int32_t* fl, int G, int n_cfg,
                       const int32_t* n_cfg_dev, double cancel_tau, bool prune, cudaStream_t st);
+// Ordered list of the items whose flags have a bit of set_mask and none of clear_mask.
 int launch_flagged(const int32_t* flags, int n_items, const int32_t* count_dev, int count_mult,
-                   int32_t* list, int32_t* count, cudaStream_t st);
+                   int32_t* list, int32_t* count, cudaStream_t st, int set_mask = NH_FLAG_GROWTH,
+                   int clear_mask = 0);
 int launch_wtilde(const float* W, float theta, int Lx, int Ly, int d, float* Wt, double* Wt64,
                   cudaStream_t st);
 // Tensor-core CNN (nh_cnn_tc.cu).

@@ -87,6 +87,8 @@ struct PfArgs {
   double cond_tau;           // flag NH_FLAG_GROWTH when max|piv| > cond_tau min|piv| (0: off)
   int flag_or;               // OR-ed into every written flag
   void* tri;                 // large n: per-CTA lower triangles of T in global memory
+  uint16_t* perm;            // or null: per item, logical -> physical row, then the parity
+  double refine_tau;         // set kFlagNeedRefine when max|piv| > refine_tau min|piv| (0: off)
 };
 
 __device__ __forceinline__ int tri_off(int i) { return (i * (i - 1)) >> 1; }
@@ -206,7 +208,7 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
     __syncthreads();
 
     int my_log = tid < n ? tid : -1;
-    int flag = 0;
+    int flag = 0, swaps = 0;
     bool zero = false;
 
     for (int k0 = 0; k0 < n - 1 && !zero; k0 += 2 * NB) {
@@ -314,6 +316,7 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
             }
             if (my_log == k + 2) misc[0] = tid;
             if (tid == 0) pivs[k >> 1] = lr != k + 1 ? -piv : piv;
+            swaps ^= lr != k + 1 ? 1 : 0;
           }
           __syncthreads();  // (2) panel column written, next column's owner known
         }
@@ -432,11 +435,18 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
         la = log(mant) + (double)expo * 0.6931471805599453;
         if (!isfinite(la)) flag |= NH_FLAG_NONFINITE;
         if (a.cond_tau > 0.0 && pmax > a.cond_tau * pmin) flag |= NH_FLAG_GROWTH;
+        if (a.refine_tau > 0.0 && pmax > a.refine_tau * pmin) flag |= kFlagNeedRefine;
       }
       if (s == 0.0f) la = -INFINITY;
       a.sign[item] = s;
       a.logabs[item] = la;
       if (a.flags) a.flags[item] = flag | a.flag_or;
+    }
+    // Pivot order for the FP64 refinement: every row's final logical label, and the parity.
+    if (a.perm && !zero) {
+      uint16_t* pr = a.perm + (size_t)item * perm_stride(n);
+      if (tid < n) pr[my_log] = (uint16_t)tid;
+      if (tid == 0) pr[n] = (uint16_t)swaps;
     }
   }
 }
@@ -700,12 +710,13 @@ __global__ void image_mark_kernel(const float* __restrict__ sg, const double* __
 __global__ void combine_kernel(const float* __restrict__ sg, const double* __restrict__ la,
                                const int32_t* __restrict__ fl, int G, int n_cfg,
                                const int32_t* n_cfg_dev, float* sign, double* logabs,
-                               int32_t* flags, double cancel_tau) {
+                               int32_t* flags, double cancel_tau, const int32_t* err) {
   const int n = n_cfg_dev ? *n_cfg_dev : n_cfg;
+  const int timeout = (err && *err) ? NH_FLAG_TIMEOUT : 0;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
-    int f = 0;
+    int f = timeout;
     if (fl)
-      for (int g = 0; g < G; ++g) f |= fl[(size_t)c * G + g];
+      for (int g = 0; g < G; ++g) f |= fl[(size_t)c * G + g] & kPublicFlags;
     double m, a;
     const double tot = image_sum(sg, la, c, G, &m, &a);
     if (cancel_tau > 0.0 && a > 0.0 && a > cancel_tau * fabs(tot)) f |= NH_FLAG_CANCEL;
@@ -716,11 +727,13 @@ __global__ void combine_kernel(const float* __restrict__ sg, const double* __res
   }
 }
 
-// Ordered list of the items whose flags carry NH_FLAG_GROWTH (single CTA).
+// Ordered list of the items whose flags carry a bit of set_mask and none of clear_mask (single
+// CTA).
 __global__ void __launch_bounds__(1024) flagged_kernel(const int32_t* __restrict__ flags,
                                                        int n_items, const int32_t* count_dev,
                                                        int count_mult, int32_t* list,
-                                                       int32_t* count) {
+                                                       int32_t* count, int set_mask,
+                                                       int clear_mask) {
   __shared__ int wsum[32];
   __shared__ int carry;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -729,7 +742,8 @@ __global__ void __launch_bounds__(1024) flagged_kernel(const int32_t* __restrict
   __syncthreads();
   for (int base = 0; base < n; base += 1024) {
     const int i = base + threadIdx.x;
-    const int v = i < n ? ((flags[i] & NH_FLAG_GROWTH) != 0) : 0;
+    const int f = i < n ? flags[i] : 0;
+    const int v = (i < n && (f & set_mask) && !(f & clear_mask)) ? 1 : 0;
     const unsigned bal = __ballot_sync(0xffffffffu, v);
     if (lane == 0) wsum[wid] = __popc(bal);
     __syncthreads();
@@ -937,7 +951,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, i
     __syncthreads();
 
     int my_log = tid < n ? tid : -1;
-    int flag = 0;
+    int flag = 0, swaps = 0;
     bool zero = false, abort = false;
     for (int k0 = 0; k0 < n - 1 && !zero && !abort; k0 += 2 * kTcNB) {
       const int steps = min(kTcNB, (n - k0) >> 1);
@@ -1019,6 +1033,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, i
             Vs[o] = tf32_big(v - vb);
             if (my_log == k + 2) misc[0] = tid;
             if (tid == 0) pivs[k >> 1] = lr != k + 1 ? -piv : piv;
+            swaps ^= lr != k + 1 ? 1 : 0;
           }
           __syncthreads();  // (2) panel column written, next column's owner known
         }
@@ -1093,11 +1108,17 @@ __global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, i
         la = log(mant) + (double)expo * 0.6931471805599453;
         if (!isfinite(la)) flag |= NH_FLAG_NONFINITE;
         if (a.cond_tau > 0.0 && pmax > a.cond_tau * pmin) flag |= NH_FLAG_GROWTH;
+        if (a.refine_tau > 0.0 && pmax > a.refine_tau * pmin) flag |= kFlagNeedRefine;
       }
       if (s == 0.0f) la = -INFINITY;
       a.sign[item] = s;
       a.logabs[item] = la;
       if (a.flags) a.flags[item] = flag | a.flag_or;
+    }
+    if (a.perm && !zero && !abort) {
+      uint16_t* pr = a.perm + (size_t)item * perm_stride(n);
+      if (tid < n) pr[my_log] = (uint16_t)tid;
+      if (tid == 0) pr[n] = (uint16_t)swaps;
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1149,7 +1170,7 @@ size_t pfaffian_scratch_bytes(int n) {
 int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list,
                            const int32_t* count, bool fp64, double cond_tau, int flag_or,
                            float* sign, double* logabs, int32_t* flags, void* tri,
-                           cudaStream_t st) {
+                           cudaStream_t st, uint16_t* perm, double refine_tau) {
   if (n <= 0 || n % 2 || n > kBigThreads)
     return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d must be even and <= %d", n, kBigThreads);
   PfArgs a{};
@@ -1166,6 +1187,8 @@ int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list
   a.cond_tau = cond_tau;
   a.flag_or = flag_or;
   a.tri = tri;
+  a.perm = perm;
+  a.refine_tau = refine_tau;
   return fp64 ? launch_pf_pick<double, 16>(a, st) : launch_pf_pick<float, 16>(a, st);
 }
 
@@ -1191,6 +1214,8 @@ int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st) {
   a.cond_tau = g.cond_tau;
   a.flag_or = g.flag_or;
   a.tri = g.tri;
+  a.perm = g.perm;
+  a.refine_tau = g.refine_tau;
   return g.fp64 ? launch_pf_d<double>(a, g.d, st) : launch_pf_d<float>(a, g.d, st);
 }
 
@@ -1218,6 +1243,8 @@ int launch_pfaffian_tc(const PfGatherArgs& g, int mode, const float* F, int32_t*
   a.flags = g.flags;
   a.cond_tau = g.cond_tau;
   a.flag_or = g.flag_or;
+  a.perm = g.perm;
+  a.refine_tau = g.refine_tau;
   switch (mode == 0 ? 16 : g.d) {
     case 8: return launch_pf_tc<8>(a, err, st);
     case 16: return launch_pf_tc<16>(a, err, st);
@@ -1269,12 +1296,12 @@ int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, 
 
 int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, int n_cfg,
                    const int32_t* n_cfg_dev, float* sign, double* logabs, int32_t* flags,
-                   double cancel_tau, cudaStream_t st) {
+                   double cancel_tau, const int32_t* err, cudaStream_t st) {
   if (n_cfg <= 0) return NH_OK;
   int grid = (n_cfg + 255) / 256;
   ProfScope prof_scope(NH_K_COMBINE, st);
   combine_kernel<<<grid, 256, 0, st>>>(sg, la, fl, G, n_cfg, n_cfg_dev, sign, logabs, flags,
-                                       G > 1 ? cancel_tau : 0.0);
+                                       G > 1 ? cancel_tau : 0.0, err);
   return check_launch("combine_kernel");
 }
 
@@ -1288,9 +1315,10 @@ int launch_image_mark(const float* sg, const double* la, int32_t* fl, int G, int
 }
 
 int launch_flagged(const int32_t* flags, int n_items, const int32_t* count_dev, int count_mult,
-                   int32_t* list, int32_t* count, cudaStream_t st) {
+                   int32_t* list, int32_t* count, cudaStream_t st, int set_mask, int clear_mask) {
   ProfScope prof_scope(NH_K_FLAGGED, st);
-  flagged_kernel<<<1, 1024, 0, st>>>(flags, n_items, count_dev, count_mult, list, count);
+  flagged_kernel<<<1, 1024, 0, st>>>(flags, n_items, count_dev, count_mult, list, count, set_mask,
+                                     clear_mask);
   return check_launch("flagged_kernel");
 }
 

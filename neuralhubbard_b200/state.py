@@ -63,10 +63,17 @@ class Variational:
     ``code/states.py:80,316-320``); the workspace for one chunk is allocated once and cached.
     """
 
-    def __init__(self, model: PfaffianBackflow, symm: bool = True, max_parallel: int = 8192):
+    def __init__(self, model: PfaffianBackflow, symm: bool = True, max_parallel: int = 8192,
+                 check_timeout: bool = True):
+        """``check_timeout`` (tensor-core forms only): read the output flags back after each call
+        and raise ``DeviceTimeoutError`` if a tensor-core kernel's bounded wait expired (one
+        small device-to-host copy; pass False to keep the call free of host synchronisation and
+        test ``LogArray.flags`` for ``FLAG_TIMEOUT`` yourself)."""
         self.model = model
         self.n_symm = 8 if symm else 1
         self.max_parallel = int(max_parallel)
+        self.check_timeout = bool(check_timeout) and (model.cnn_mode in (1, 2)
+                                                      or model.pf_mode == 1)
 
     @property
     def device(self):
@@ -95,4 +102,6 @@ class Variational:
             _lib.call("nh_amplitude", spins[c0:c1].data_ptr(), c1 - c0, self.n_symm,
                       ctypes.byref(p), sign[c0:].data_ptr(), logabs[c0:].data_ptr(),
                       flags[c0:].data_ptr(), ws.data_ptr(), ws.numel(), st)
+        if self.check_timeout:
+            _lib.check_flags(flags, "nh_amplitude")
         return LogArray(sign, logabs, flags)

@@ -65,19 +65,20 @@ def test_argument_checks_before_device_work():
     lib = _lib.load()
     p = ctypes.c_void_p(4096)
 
-    def slogpf(n, flags=p, ws=p, nbytes=1 << 20, tau=100.0):
+    def slogpf(n, flags=p, ws=p, nbytes=1 << 26, tau=100.0):
         return lib.nh_slogpf(p, n, 4, tau, p, p, flags, ws, nbytes, None)
 
     assert slogpf(7) == -2 and b"must be even" in lib.nh_last_error()
     assert slogpf(1026) == -2
-    assert lib.nh_slogpf(None, 56, 4, 100.0, p, p, p, p, 1 << 20, None) == -1
+    assert lib.nh_slogpf(None, 56, 4, 100.0, p, p, p, p, 1 << 26, None) == -1
     assert slogpf(56, flags=None) == -1 and b"needs flags" in lib.nh_last_error()
     assert slogpf(56, nbytes=16) == -4
     assert slogpf(56, ws=None) == -4
     assert slogpf(56, ws=ctypes.c_void_p(4096 + 16)) == -1
     assert b"256-byte aligned" in lib.nh_last_error()
     assert lib.nh_slogpf_noalloc(p, 300, 4, 100.0, p, p, p, None) == -2
-    assert lib.nh_slogpf_workspace_bytes(56, 4) == lib.nh_slogpf_workspace_bytes(56, 64)
+    # 256-byte granularity: one and two matrices need the same workspace, more need more
+    assert lib.nh_slogpf_workspace_bytes(56, 1) == lib.nh_slogpf_workspace_bytes(56, 2)
     assert lib.nh_slogpf_workspace_bytes(56, 65) > lib.nh_slogpf_workspace_bytes(56, 64)
 
 
@@ -187,3 +188,24 @@ def test_residual_network_argument_checks():
     assert amplitude(cnn_mode=1) == -2
     assert amplitude(cnn_mode=2, Lx=8, Ly=8, n_up=28, n_dn=28) == -2
     assert amplitude(net=7) == -1 and b"net 7" in lib.nh_last_error()
+
+
+def test_timeout_flag_raises():
+    """NH_FLAG_TIMEOUT (a tensor-core kernel's bounded wait expired; the combination folds the
+    device error word into every output flag) must surface as an exception in the host layer,
+    and flags without it must pass."""
+    import numpy as np
+
+    from neuralhubbard_b200 import _lib
+
+    ok = np.array([0, _lib.FLAG_REFINED, _lib.FLAG_GROWTH | _lib.FLAG_CANCEL], np.int32)
+    _lib.check_flags(ok, "test")
+    assert not _lib.timeout_flagged(ok)
+    bad = ok | _lib.FLAG_TIMEOUT
+    assert _lib.timeout_flagged(bad)
+    with pytest.raises(_lib.DeviceTimeoutError):
+        _lib.check_flags(bad, "test")
+    import torch
+
+    with pytest.raises(_lib.DeviceTimeoutError):
+        _lib.check_flags(torch.from_numpy(bad), "test")
