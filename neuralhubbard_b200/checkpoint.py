@@ -65,10 +65,17 @@ def file_md5(path: str) -> str:
         return hashlib.md5(f.read()).hexdigest()
 
 
-def load_pfaffian_backflow(path: str, L: Optional[int] = None) -> dict:
+def load_pfaffian_backflow(path: str, L: Optional[int] = None,
+                           expect_md5: Optional[str] = None) -> dict:
     """Parameters of a released Pfaffian-backflow state as the dict ``PfaffianBackflow``
     takes: ``net="resconv"``, ``embed`` (C, 4), ``conv_w`` / ``conv_b`` (2 * blocks arrays,
-    block order), ``W`` (3, N, d), ``theta``.  ``L`` checks the lattice size."""
+    block order), ``W`` (3, N, d), ``theta``.  ``L`` checks the lattice size; ``expect_md5``
+    (e.g. ``RELEASED[name].md5``) checks the file's checksum first, as the reference does
+    before loading (``code/states.py:308-311``), and raises ``CheckpointError`` on a mismatch."""
+    if expect_md5 is not None:
+        got = file_md5(path)
+        if got != expect_md5:
+            raise CheckpointError(f"{path}: md5 {got}, expected {expect_md5}")
     leaves = read_leaves(path)
     floats = [a for a in leaves if a.dtype == np.float32]
     if len(floats) < 5 or floats[0].ndim != 4 or floats[0].shape[1:] != (4, 1, 1):
@@ -100,12 +107,24 @@ def load_pfaffian_backflow(path: str, L: Optional[int] = None) -> dict:
                 conv_b=conv_b, W=np.ascontiguousarray(W), theta=float(theta))
 
 
-def load_spins(path: str, N: Optional[int] = None) -> np.ndarray:
-    """Equilibrated chains as int8 +-1 (nchains, 2N), spin-up sites first."""
+def load_spins(path: str, N: Optional[int] = None, n_up: Optional[int] = None,
+               n_dn: Optional[int] = None) -> np.ndarray:
+    """Equilibrated chains as int8 +-1 (nchains, 2N), spin-up sites first.  With ``n_up`` /
+    ``n_dn`` every chain's particle numbers are checked, as the reference does for its stored
+    chains (``code/states.py:346-351``); a mismatch raises ``CheckpointError``."""
     with np.load(path) as f:
         bits, shape = f["bits"], tuple(int(x) for x in f["shape"])
     s = np.unpackbits(bits, axis=-1, count=shape[-1]).astype(np.int8)
     s = (2 * s - 1).reshape(shape)
     if N is not None and s.shape[1] != 2 * N:
         raise CheckpointError(f"{path}: configurations of length {s.shape[1]}, not {2 * N}")
+    half = s.shape[1] // 2
+    for want, part, name in ((n_up, s[:, :half], "up"), (n_dn, s[:, half:], "down")):
+        if want is None:
+            continue
+        got = (part > 0).sum(1)
+        bad = np.nonzero(got != want)[0]
+        if bad.size:
+            raise CheckpointError(f"{path}: chain {int(bad[0])} holds {int(got[bad[0]])} spin-"
+                                  f"{name} electrons, not {want} ({bad.size} chains differ)")
     return s

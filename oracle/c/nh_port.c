@@ -255,34 +255,36 @@ int nhp_amplitudes(const int8_t* spins, int B, int Lx, int Ly, int C, int layers
     w.occ = malloc(sizeof(int) * (size_t)n);
     w.img = malloc((size_t)2 * N);
     int* occs = malloc(sizeof(int) * (size_t)2 * N);
-    if (!w.act[0] || !w.act[1] || !w.Y || !w.A || !w.tmp || !w.xyz || !w.occ || !w.img ||
-        !occs) {
+    const int ok = w.act[0] && w.act[1] && w.Y && w.A && w.tmp && w.xyz && w.occ && w.img && occs;
+    if (!ok) {
 #pragma omp atomic write
       err = -2;
-    } else {
+    }
+    /* Every thread meets the worksharing loop (an OpenMP requirement); a thread whose buffers
+       are missing takes its share of iterations without computing them (err is set). */
 #pragma omp for schedule(dynamic, 1)
-      for (int b = 0; b < B; ++b) {
-        const int8_t* s = spins + (size_t)b * 2 * N;
-        int k = 0;
-        for (int m = 0; m < 2 * N; ++m)
-          if (s[m] > 0) occs[k++] = m;
-        double mx = -INFINITY, sg[64], la[64];
-        for (int g = 0; g < G && g < 64; ++g) {
-          const int64_t* mp = maps + (size_t)g * 2 * N;
-          for (int m = 0; m < 2 * N; ++m) w.img[mp[m]] = s[m];
-          int inv = 0; /* eta_g: parity of sorting the mapped occupied modes */
-          for (int i = 0; i < k; ++i)
-            for (int j = i + 1; j < k; ++j) inv += mp[occs[i]] > mp[occs[j]];
-          amplitude(&net, &w, w.img, &sg[g], &la[g]);
-          if (inv & 1) sg[g] = -sg[g];
-          if (sg[g] != 0.0 && la[g] > mx) mx = la[g];
-        }
-        if (!isfinite(mx)) mx = 0.0;
-        double tot = 0.0;
-        for (int g = 0; g < G && g < 64; ++g) tot += sg[g] * exp(la[g] - mx);
-        sign[b] = tot > 0 ? 1.0 : (tot < 0 ? -1.0 : 0.0);
-        logabs[b] = log(fabs(tot)) + mx - log((double)G);
+    for (int b = 0; b < B; ++b) {
+      if (!ok) continue;
+      const int8_t* s = spins + (size_t)b * 2 * N;
+      int k = 0;
+      for (int m = 0; m < 2 * N; ++m)
+        if (s[m] > 0) occs[k++] = m;
+      double mx = -INFINITY, sg[64], la[64];
+      for (int g = 0; g < G && g < 64; ++g) {
+        const int64_t* mp = maps + (size_t)g * 2 * N;
+        for (int m = 0; m < 2 * N; ++m) w.img[mp[m]] = s[m];
+        int inv = 0; /* eta_g: parity of sorting the mapped occupied modes */
+        for (int i = 0; i < k; ++i)
+          for (int j = i + 1; j < k; ++j) inv += mp[occs[i]] > mp[occs[j]];
+        amplitude(&net, &w, w.img, &sg[g], &la[g]);
+        if (inv & 1) sg[g] = -sg[g];
+        if (sg[g] != 0.0 && la[g] > mx) mx = la[g];
       }
+      if (!isfinite(mx)) mx = 0.0;
+      double tot = 0.0;
+      for (int g = 0; g < G && g < 64; ++g) tot += sg[g] * exp(la[g] - mx);
+      sign[b] = tot > 0 ? 1.0 : (tot < 0 ? -1.0 : 0.0);
+      logabs[b] = log(fabs(tot)) + mx - log((double)G);
     }
     free(w.act[0]);
     free(w.act[1]);

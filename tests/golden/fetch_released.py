@@ -1,9 +1,10 @@
 """Copy the released 16x16 Pfaffian-backflow state (parameters and equilibrated chains) from a
 checkout of the reference into tests/golden/released/, checking the parameter file's md5.
 
-    python tests/golden/fetch_released.py [REFERENCE_ROOT] [NAME ...]
+    python tests/golden/fetch_released.py REFERENCE_ROOT [NAME ...]
 
-REFERENCE_ROOT defaults to /root/reference; NAME to tpm02_L16_pfaffian.  The copies are not
+REFERENCE_ROOT is the root of a ChenAo-Phys/NeuralHubbard checkout (it holds weights/); NAME
+defaults to tpm02_L16_pfaffian.  The copies are not
 committed (tests/golden/released/ is git-ignored: 5 MB of weights); tests that need them skip
 when they are absent.
 """
@@ -19,7 +20,9 @@ from neuralhubbard_b200 import checkpoint  # noqa: E402
 
 
 def main(argv):
-    root = argv[1] if len(argv) > 1 else "/root/reference"
+    if len(argv) < 2:
+        raise SystemExit(__doc__)
+    root = argv[1]
     names = argv[2:] or ["tpm02_L16_pfaffian"]
     out = os.path.join(HERE, "released")
     os.makedirs(out, exist_ok=True)
