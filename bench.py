@@ -137,11 +137,12 @@ def _cpu_worker(args):
     return time.perf_counter() - t0
 
 
-def cpu_baseline(target_s: float = 12.0) -> dict:
+def cpu_baseline(target_s: float = 12.0, fp32: bool = True) -> dict:
     """Projected amplitudes of the same workload by the CPU restatement on all host cores, on a
     bounded sample sized for ~target_s seconds: the compiled restatement (oracle/c/nh_port.c,
-    gcc -O3, OpenMP across configurations) when it builds, else the numpy oracle in a spawn
-    pool (one numpy thread per core)."""
+    gcc -O3, OpenMP across configurations; its FP32 build by default, the arithmetic of the
+    reference's own path, or the FP64 build) when it builds, else the numpy oracle (FP64) in a
+    spawn pool (one numpy thread per core)."""
     import multiprocessing as mp
 
     from neuralhubbard_b200.backflow import init_params
@@ -159,23 +160,24 @@ def cpu_baseline(target_s: float = 12.0) -> dict:
     try:
         from oracle import port
 
-        port.load()
+        port.load(fp32)
     except Exception:
         port = None
     if port is not None:
         warm = random_spins(rng, cores, N_SITES, NE, NE)
         t0 = time.perf_counter()
-        port.projected_amplitude(warm, params, threads=cores)
+        port.projected_amplitude(warm, params, threads=cores, fp32=fp32)
         t_batch = time.perf_counter() - t0
         n_cfg = max(cores, int(cores * target_s / max(t_batch, 1e-3)))
         sample = random_spins(rng, n_cfg, N_SITES, NE, NE)
         t0 = time.perf_counter()
-        port.projected_amplitude(sample, params, threads=cores)
+        port.projected_amplitude(sample, params, threads=cores, fp32=fp32)
         wall = time.perf_counter() - t0
         n_amp = n_cfg * IMAGES
+        prec = "FP32" if fp32 else "FP64"
         return {"value": n_amp / wall, "unit": UNIT, "cores": cores, "kind": "port",
                 "sample": f"{n_cfg} configurations x {IMAGES} images at 16x16 ({n_amp} "
-                          f"amplitudes, compiled FP64 restatement, gcc -O3 + OpenMP, "
+                          f"amplitudes, compiled {prec} restatement, gcc -O3 + OpenMP, "
                           f"{wall:.1f} s)",
                 "seconds": wall}
     for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
@@ -800,7 +802,12 @@ def run_ours(args) -> None:
         released_sampling = measure_released_sampling(args, dev, st)
 
     if rank == 0:
-        cpu = cpu_baseline() if world == 1 and not args.no_cpu_baseline else None
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            # FP32 (the reference's arithmetic) is the baseline; FP64 rides along for comparison.
+            cpu = cpu_baseline(fp32=True)
+            c64 = cpu_baseline(target_s=8.0, fp32=False)
+            cpu["fp64"] = {"value": c64["value"], "sample": c64["sample"]}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -849,12 +856,13 @@ def run_reference(args) -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
         "data": "synthetic",
         "config": {"workload": "projected amplitudes, 16x16 Hubbard lattice, 112+112 electrons, "
                                "8 images per configuration (bounded sample per step)",
-                   "form": "compiled CPU restatement of the reference path (C, FP64, OpenMP "
-                           "across configurations; the JAX stack is not installable)",
+                   "form": "compiled CPU restatement of the reference path (C, FP32 like the "
+                           "reference's own arithmetic, OpenMP across configurations; the JAX "
+                           "stack is not installable)",
                    "L": L, "images": IMAGES},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": last["cores"], "kind": "port",
                          "sample": last["sample"]},
@@ -878,13 +886,12 @@ def run_reference(args) -> None:
 #   refine             16x16 projected amplitudes, 512 x 8 images, every image refined in FP64
 
 def _model(L, cnn_mode=0):
-    import torch
 
     import neuralhubbard_b200 as nh
 
     ne = 7 * L * L // 16
-    return nh.PfaffianBackflow(L, L, ne, ne, params=nh.init_params(L, L, 32, 4, std=0.02, seed=0),
-                            cnn_mode=cnn_mode), ne
+    params = nh.init_params(L, L, 32, 4, std=0.02, seed=0)
+    return nh.PfaffianBackflow(L, L, ne, ne, params=params, cnn_mode=cnn_mode), ne
 
 
 def case_pairing(repeat):

@@ -23,74 +23,90 @@
 #include <omp.h>
 #endif
 
+/* Arithmetic type: double by default; the FP32 build (-DNHP_FP32) computes the CNN, the gather
+ * and the Parlett-Reid updates in float, the precision of the reference's own JAX path
+ * (FP32 with TF32 convolutions), and exports nhp_amplitudes_f32.  The log-sum of the pivots and
+ * of the images stays in double in both builds. */
+#ifdef NHP_FP32
+typedef float real;
+#define RTANH tanhf
+#define RFABS fabsf
+#define NHP_ENTRY nhp_amplitudes_f32
+#else
+typedef double real;
+#define RTANH tanh
+#define RFABS fabs
+#define NHP_ENTRY nhp_amplitudes
+#endif
+
 typedef struct {
   int Lx, Ly, N, C, layers, d, n, G;
-  const double* conv_w; /* layers concatenated: (C_out, C_in, 3, 3), C_in = 2 for layer 0 */
-  const double* conv_b; /* (layers, C) */
-  const double* Wt;     /* (4, N, d) */
+  const real* conv_w; /* layers concatenated: (C_out, C_in, 3, 3), C_in = 2 for layer 0 */
+  const real* conv_b; /* (layers, C) */
+  const real* Wt;     /* (4, N, d) */
   const int64_t* maps;  /* (G, 2N) */
 } Net;
 
 typedef struct {
-  double* act[2]; /* padded planes (C, Lx + 2, Ly + 2) */
-  double* Y;      /* (n, d) */
-  double* A;      /* (n, n) */
-  double* tmp;    /* (2n) Pfaffian row buffers */
+  real* act[2]; /* padded planes (C, Lx + 2, Ly + 2) */
+  real* Y;      /* (n, d) */
+  real* A;      /* (n, n) */
+  real* tmp;    /* (2n) Pfaffian row buffers */
   int* xyz;       /* (3n) x, y, spin of each occupied mode */
   int* occ;       /* (n) occupied modes of the image */
   int8_t* img;    /* (2N) */
 } Work;
 
-static double gelu_tanh(double x) {
-  const double k0 = 0.7978845608028654; /* sqrt(2 / pi) */
-  return 0.5 * x * (1.0 + tanh(k0 * (x + 0.044715 * x * x * x)));
+static real gelu_tanh(real x) {
+  const real k0 = (real)0.7978845608028654; /* sqrt(2 / pi) */
+  return (real)0.5 * x * ((real)1 + RTANH(k0 * (x + (real)0.044715 * x * x * x)));
 }
 
 /* Periodic halo of one padded plane. */
-static void fill_halo(double* p, int Lx, int Ly) {
+static void fill_halo(real* p, int Lx, int Ly) {
   const int P = Ly + 2;
   for (int x = 1; x <= Lx; ++x) {
     p[x * P] = p[x * P + Ly];
     p[x * P + Ly + 1] = p[x * P + 1];
   }
-  memcpy(p, p + Lx * P, sizeof(double) * P);
-  memcpy(p + (Lx + 1) * P, p + P, sizeof(double) * P);
+  memcpy(p, p + Lx * P, sizeof(real) * P);
+  memcpy(p + (Lx + 1) * P, p + P, sizeof(real) * P);
 }
 
 /* Features of the image configuration: the last layer's channels, act[out] (C planes). */
 static int cnn(const Net* net, Work* w, const int8_t* s) {
   const int Lx = net->Lx, Ly = net->Ly, N = net->N, C = net->C, P = Ly + 2;
   const int plane = (Lx + 2) * P;
-  double* in = w->act[0];
-  double* out = w->act[1];
+  real* in = w->act[0];
+  real* out = w->act[1];
   for (int ch = 0; ch < 2; ++ch) {
-    double* p = in + ch * plane;
+    real* p = in + ch * plane;
     for (int x = 0; x < Lx; ++x)
-      for (int y = 0; y < Ly; ++y) p[(x + 1) * P + y + 1] = s[ch * N + x * Ly + y] > 0 ? 1.0 : -1.0;
+      for (int y = 0; y < Ly; ++y) p[(x + 1) * P + y + 1] = s[ch * N + x * Ly + y] > 0 ? (real)1 : (real)-1;
     fill_halo(p, Lx, Ly);
   }
-  const double* wl = net->conv_w;
+  const real* wl = net->conv_w;
   int cin = 2;
   for (int l = 0; l < net->layers; ++l) {
-    const double* bl = net->conv_b + (size_t)l * C;
+    const real* bl = net->conv_b + (size_t)l * C;
     /* Four output channels at a time: each input row is loaded once for four FMA streams. */
     for (int o0 = 0; o0 < C; o0 += 4) {
       const int no = C - o0 < 4 ? C - o0 : 4;
       for (int x = 0; x < Lx; ++x) {
-        double acc[4][64];
+        real acc[4][64];
         for (int j = 0; j < no; ++j)
           for (int y = 0; y < Ly; ++y) acc[j][y] = bl[o0 + j];
         for (int i = 0; i < cin; ++i) {
-          const double* pi = in + i * plane;
+          const real* pi = in + i * plane;
           for (int u = 0; u < 3; ++u) {
-            const double* srow = pi + (x + u) * P;
+            const real* srow = pi + (x + u) * P;
             for (int v = 0; v < 3; ++v) {
-              const double* src = srow + v;
-              double wv[4];
+              const real* src = srow + v;
+              real wv[4];
               for (int j = 0; j < 4; ++j)
-                wv[j] = j < no ? wl[((size_t)(o0 + j) * cin + i) * 9 + u * 3 + v] : 0.0;
+                wv[j] = j < no ? wl[((size_t)(o0 + j) * cin + i) * 9 + u * 3 + v] : (real)0;
               for (int y = 0; y < Ly; ++y) {
-                const double sv = src[y];
+                const real sv = src[y];
                 acc[0][y] += wv[0] * sv;
                 acc[1][y] += wv[1] * sv;
                 acc[2][y] += wv[2] * sv;
@@ -100,7 +116,7 @@ static int cnn(const Net* net, Work* w, const int8_t* s) {
           }
         }
         for (int j = 0; j < no; ++j) {
-          double* dst = out + (o0 + j) * plane + (x + 1) * P + 1;
+          real* dst = out + (o0 + j) * plane + (x + 1) * P + 1;
           if (l < net->layers - 1)
             for (int y = 0; y < Ly; ++y) dst[y] = gelu_tanh(acc[j][y]);
           else
@@ -111,21 +127,21 @@ static int cnn(const Net* net, Work* w, const int8_t* s) {
     for (int o = 0; o < C; ++o) fill_halo(out + o * plane, Lx, Ly);
     wl += (size_t)C * cin * 9;
     cin = C;
-    double* t = in;
+    real* t = in;
     in = out;
     out = t;
   }
   return in == w->act[0] ? 0 : 1;
 }
 
-/* (sign, log|pf|) of the antisymmetric n x n matrix A (destroyed); tmp holds 2n doubles. */
-static void slogpf(double* A, int n, double* tmp, double* sign, double* logabs) {
+/* (sign, log|pf|) of the antisymmetric n x n matrix A (destroyed); tmp holds 2n values. */
+static void slogpf(real* A, int n, real* tmp, double* sign, double* logabs) {
   double sg = 1.0, la = 0.0;
   for (int k = 0; k + 1 < n; k += 2) {
     int kp = k + 1;
-    double best = fabs(A[(size_t)(k + 1) * n + k]);
+    real best = RFABS(A[(size_t)(k + 1) * n + k]);
     for (int i = k + 2; i < n; ++i) {
-      const double v = fabs(A[(size_t)i * n + k]);
+      const real v = RFABS(A[(size_t)i * n + k]);
       if (v > best) {
         best = v;
         kp = i;
@@ -133,36 +149,36 @@ static void slogpf(double* A, int n, double* tmp, double* sign, double* logabs) 
     }
     if (kp != k + 1) { /* swap rows and columns k + 1 and kp */
       for (int j = 0; j < n; ++j) {
-        const double t = A[(size_t)(k + 1) * n + j];
+        const real t = A[(size_t)(k + 1) * n + j];
         A[(size_t)(k + 1) * n + j] = A[(size_t)kp * n + j];
         A[(size_t)kp * n + j] = t;
       }
       for (int i = 0; i < n; ++i) {
-        const double t = A[(size_t)i * n + k + 1];
+        const real t = A[(size_t)i * n + k + 1];
         A[(size_t)i * n + k + 1] = A[(size_t)i * n + kp];
         A[(size_t)i * n + kp] = t;
       }
       sg = -sg;
     }
-    const double piv = A[(size_t)k * n + k + 1];
-    if (piv == 0.0) {
+    const real piv = A[(size_t)k * n + k + 1];
+    if (piv == (real)0) {
       *sign = 0.0;
       *logabs = -INFINITY;
       return;
     }
     sg *= piv > 0 ? 1.0 : -1.0;
-    la += log(fabs(piv));
+    la += log(fabs((double)piv));
     /* A[k+2:, k+2:] += tau a^T - a tau^T, tau = A[k, k+2:] / piv, a = A[k+2:, k+1], with tau
      * and a copied into contiguous buffers so that the row updates vectorise. */
-    double* tau = tmp;
-    double* acol = tmp + n;
+    real* tau = tmp;
+    real* acol = tmp + n;
     for (int j = k + 2; j < n; ++j) {
       tau[j] = A[(size_t)k * n + j] / piv;
       acol[j] = A[(size_t)j * n + k + 1];
     }
     for (int i = k + 2; i < n; ++i) {
-      const double ti = tau[i], ai = acol[i];
-      double* row = A + (size_t)i * n;
+      const real ti = tau[i], ai = acol[i];
+      real* row = A + (size_t)i * n;
       for (int j = k + 2; j < n; ++j) row[j] += ti * acol[j] - ai * tau[j];
     }
   }
@@ -185,7 +201,7 @@ static void amplitude(const Net* net, Work* w, const int8_t* img, double* sign, 
     *logabs = -INFINITY;
     return;
   }
-  const double* feat = w->act[cnn(net, w, img)];
+  const real* feat = w->act[cnn(net, w, img)];
   for (int p = 0; p < n; ++p) {
     const int m = w->occ[p], sp = m >= N, site = m - sp * N;
     const int x = site / Ly, y = site - x * Ly;
@@ -202,7 +218,7 @@ static void amplitude(const Net* net, Work* w, const int8_t* img, double* sign, 
   }
   for (int p = 0; p < n; ++p) {
     const int sp = S[p], xp = X[p], yp = Yc[p];
-    w->A[(size_t)p * n + p] = 0.0;
+    w->A[(size_t)p * n + p] = 0;
     for (int q = 0; q < p; ++q) {
       const int sq = S[q];
       int dx = xp - X[q], dy = yp - Yc[q];
@@ -210,15 +226,15 @@ static void amplitude(const Net* net, Work* w, const int8_t* img, double* sign, 
       dy += dy < 0 ? Ly : 0;
       const int r = dx * Ly + dy;
       const int rn = (dx ? Lx - dx : 0) * Ly + (dy ? Ly - dy : 0);
-      const double* wpq = net->Wt + ((size_t)(2 * sp + sq) * N + r) * d;
-      const double* wqp = net->Wt + ((size_t)(2 * sq + sp) * N + rn) * d;
-      double fpq = 0.0, fqp = 0.0;
+      const real* wpq = net->Wt + ((size_t)(2 * sp + sq) * N + r) * d;
+      const real* wqp = net->Wt + ((size_t)(2 * sq + sp) * N + rn) * d;
+      real fpq = 0, fqp = 0;
       for (int a = 0; a < d; ++a) {
-        const double yy = w->Y[p * d + a] * w->Y[q * d + a];
+        const real yy = w->Y[p * d + a] * w->Y[q * d + a];
         fpq += yy * wpq[a];
         fqp += yy * wqp[a];
       }
-      const double f = 0.5 * (fpq - fqp);
+      const real f = (real)0.5 * (fpq - fqp);
       w->A[(size_t)p * n + q] = f;
       w->A[(size_t)q * n + p] = -f;
     }
@@ -228,13 +244,28 @@ static void amplitude(const Net* net, Work* w, const int8_t* img, double* sign, 
 }
 
 /* Projected (G = 8) or plain (G = 1, identity map) amplitudes of B configurations. */
-int nhp_amplitudes(const int8_t* spins, int B, int Lx, int Ly, int C, int layers,
-                   const double* conv_w, const double* conv_b, const double* Wt, int n,
-                   const int64_t* maps, int G, double* sign, double* logabs, int nthreads) {
+int NHP_ENTRY(const int8_t* spins, int B, int Lx, int Ly, int C, int layers,
+              const double* conv_w, const double* conv_b, const double* Wt, int n,
+              const int64_t* maps, int G, double* sign, double* logabs, int nthreads) {
   if (!spins || !conv_w || !conv_b || !Wt || !maps || !sign || !logabs || B < 0 || G < 1 ||
       C < 2 || C % 2 || layers < 1 || n < 2 || Ly > 64 || G > 64)
     return -1; /* (the row accumulators hold 64 sites, the image sums 64 images) */
+  /* Parameters in the arithmetic type (a copy in the FP32 build). */
+  size_t n_w = 0;
+  for (int l = 0, cin = 2; l < layers; ++l, cin = C) n_w += (size_t)C * cin * 9;
+  const size_t n_b = (size_t)layers * C, n_t = (size_t)4 * Lx * Ly * (C / 2);
+#ifdef NHP_FP32
+  real* pw = malloc(sizeof(real) * (n_w + n_b + n_t));
+  if (!pw) return -2;
+  for (size_t i = 0; i < n_w; ++i) pw[i] = (real)conv_w[i];
+  for (size_t i = 0; i < n_b; ++i) pw[n_w + i] = (real)conv_b[i];
+  for (size_t i = 0; i < n_t; ++i) pw[n_w + n_b + i] = (real)Wt[i];
+  Net net = {Lx, Ly, Lx * Ly, C, layers, C / 2, n, G, pw, pw + n_w, pw + n_w + n_b, maps};
+#else
+  (void)n_t;
+  (void)n_b;
   Net net = {Lx, Ly, Lx * Ly, C, layers, C / 2, n, G, conv_w, conv_b, Wt, maps};
+#endif
   const int N = net.N;
   int err = 0;
 #ifdef _OPENMP
@@ -246,11 +277,11 @@ int nhp_amplitudes(const int8_t* spins, int B, int Lx, int Ly, int C, int layers
   {
     Work w;
     const size_t plane = (size_t)(Lx + 2) * (Ly + 2);
-    w.act[0] = malloc(sizeof(double) * plane * (C > 2 ? C : 2));
-    w.act[1] = malloc(sizeof(double) * plane * (C > 2 ? C : 2));
-    w.Y = malloc(sizeof(double) * (size_t)n * net.d);
-    w.A = malloc(sizeof(double) * (size_t)n * n);
-    w.tmp = malloc(sizeof(double) * (size_t)2 * n);
+    w.act[0] = malloc(sizeof(real) * plane * (C > 2 ? C : 2));
+    w.act[1] = malloc(sizeof(real) * plane * (C > 2 ? C : 2));
+    w.Y = malloc(sizeof(real) * (size_t)n * net.d);
+    w.A = malloc(sizeof(real) * (size_t)n * n);
+    w.tmp = malloc(sizeof(real) * (size_t)2 * n);
     w.xyz = malloc(sizeof(int) * (size_t)3 * n);
     w.occ = malloc(sizeof(int) * (size_t)n);
     w.img = malloc((size_t)2 * N);
@@ -296,5 +327,8 @@ int nhp_amplitudes(const int8_t* spins, int B, int Lx, int Ly, int C, int layers
     free(w.img);
     free(occs);
   }
+#ifdef NHP_FP32
+  free(pw);
+#endif
   return err;
 }

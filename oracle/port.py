@@ -22,16 +22,23 @@ SRC = os.path.join(HERE, "c", "nh_port.c")
 # whose /proc/cpuinfo lists those instruction sets (the built files travel to other hosts).
 LIBS = {"x86-64-v2": os.path.join(HERE, "libnh_port.so"),
         "x86-64-v3": os.path.join(HERE, "libnh_port_avx2.so")}
+# The FP32 builds (-DNHP_FP32): the same algorithm in float, the arithmetic of the reference's own
+# JAX path, for a like-for-like CPU baseline.
+LIBS32 = {"x86-64-v2": os.path.join(HERE, "libnh_port_f32.so"),
+          "x86-64-v3": os.path.join(HERE, "libnh_port_f32_avx2.so")}
 CFLAGS = ["-O3", "-fopenmp", "-fPIC", "-shared"]
 
 _lib = None
+_lib32 = None
 
 
 def build(force: bool = False) -> None:
-    """Compile the C restatement with gcc into ``oracle/libnh_port*.so``."""
-    for march, lib in LIBS.items():
-        if force or not os.path.exists(lib) or os.path.getmtime(lib) < os.path.getmtime(SRC):
-            subprocess.check_call(["gcc", *CFLAGS, f"-march={march}", SRC, "-o", lib, "-lm"])
+    """Compile the C restatement with gcc into ``oracle/libnh_port*.so`` (FP64 and FP32)."""
+    for libs, extra in ((LIBS, []), (LIBS32, ["-DNHP_FP32"])):
+        for march, lib in libs.items():
+            if force or not os.path.exists(lib) or os.path.getmtime(lib) < os.path.getmtime(SRC):
+                subprocess.check_call(["gcc", *CFLAGS, *extra, f"-march={march}", SRC, "-o", lib,
+                                       "-lm"])
 
 
 def _host_has_avx2_fma() -> bool:
@@ -42,24 +49,32 @@ def _host_has_avx2_fma() -> bool:
     return all(f" {f}" in flags for f in ("avx2", "fma", "bmi2", "movbe"))
 
 
-def load():
-    global _lib
-    if _lib is None:
+def load(fp32: bool = False):
+    """The compiled library (FP64, or the FP32 build) for this host's instruction set."""
+    global _lib, _lib32
+    if (_lib32 if fp32 else _lib) is None:
         build()
-        lib = ctypes.CDLL(LIBS["x86-64-v3" if _host_has_avx2_fma() else "x86-64-v2"])
+        march = "x86-64-v3" if _host_has_avx2_fma() else "x86-64-v2"
+        lib = ctypes.CDLL((LIBS32 if fp32 else LIBS)[march])
+        fn = lib.nhp_amplitudes_f32 if fp32 else lib.nhp_amplitudes
         p = ctypes.c_void_p
-        lib.nhp_amplitudes.restype = ctypes.c_int
-        lib.nhp_amplitudes.argtypes = [p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                                       ctypes.c_int, p, p, p, ctypes.c_int, p, ctypes.c_int, p, p,
-                                       ctypes.c_int]
-        _lib = lib
-    return _lib
+        fn.restype = ctypes.c_int
+        fn.argtypes = [p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                       p, p, p, ctypes.c_int, p, ctypes.c_int, p, p, ctypes.c_int]
+        if fp32:
+            _lib32 = lib
+        else:
+            _lib = lib
+    return _lib32 if fp32 else _lib
 
 
-def projected_amplitude(s: np.ndarray, params: dict, symm: bool = True, threads: int = 0):
-    """(sign, logabs) of psi_P(s) (or psi(s) when ``symm`` is False) for s (B, 2N), FP64; the
+def projected_amplitude(s: np.ndarray, params: dict, symm: bool = True, threads: int = 0,
+                        fp32: bool = False):
+    """(sign, logabs) of psi_P(s) (or psi(s) when ``symm`` is False) for s (B, 2N), FP64 (or
+    the FP32 build's arithmetic with ``fp32``); the
     same ``params`` dict as the numpy oracle (conv_w, conv_b lists, W, theta, Lx, Ly)."""
-    lib = load()
+    lib = load(fp32)
+    fn = lib.nhp_amplitudes_f32 if fp32 else lib.nhp_amplitudes
     s = np.ascontiguousarray(s, dtype=np.int8)
     B, M = s.shape
     Lx, Ly = params["Lx"], params["Ly"]
@@ -75,7 +90,7 @@ def projected_amplitude(s: np.ndarray, params: dict, symm: bool = True, threads:
     n = int((s[0] > 0).sum()) if B else 2
     sign = np.empty(B)
     logabs = np.empty(B)
-    rc = lib.nhp_amplitudes(s.ctypes.data, B, Lx, Ly, C, len(params["conv_w"]),
+    rc = fn(s.ctypes.data, B, Lx, Ly, C, len(params["conv_w"]),
                             conv_w.ctypes.data, conv_b.ctypes.data, Wt.ctypes.data, n,
                             maps.ctypes.data, maps.shape[0], sign.ctypes.data,
                             logabs.ctypes.data, int(threads))

@@ -84,3 +84,19 @@ def test_noalloc_rejects_large_n():
                                ctypes.c_void_p(8), ctypes.c_void_p(8), None)
     assert rc == -2
     assert b"nh_slogpf with a workspace" in lib.nh_last_error()
+
+
+def test_noalloc_beyond_fp64_shared_memory_keeps_fp32():
+    """For 236 < n <= 256 an FP64 triangle no longer fits in shared memory and this entry point
+    has no workspace for one: ill-conditioned matrices are flagged NH_FLAG_GROWTH but keep their
+    FP32 result (no NH_FLAG_REFINED), bit for bit the result of nh_slogpf without refinement."""
+    n, B = 240, 8
+    rng = np.random.default_rng(n)
+    F = torch.from_numpy(_batch(rng, n, B)).cuda()
+    s0, l0, _ = _run("nh_slogpf", F, n, B, 0.0, True)
+    for _ in range(2):
+        s1, l1, f1 = _run("nh_slogpf_noalloc", F, n, B, 100.0, False)
+        assert np.all(f1[:4] & _lib.FLAG_GROWTH)  # the four near-nodal matrices
+        assert not np.any(f1 & _lib.FLAG_REFINED)
+        assert np.array_equal(s1, s0)
+        assert np.array_equal(l1, l0)
