@@ -17,6 +17,8 @@
  *                           quantax Variational.__call__(spins) -> LogArray (sign, logabs)
  *   nh_local_energy      <- code/quick_start.py:33               H.Oloc(state, Samples(spins, psi))
  *   nh_metropolis_steps  <- code/states.py:397-408               ParticleHop ... sweep()
+ *   nh_metropolis_steps_mixed <- code/states.py:397-408          MixSampler([ParticleHop,
+ *                                                                 SiteExchange]) ... sweep()
  *   nh_metropolis_steps_learned, nh_proposal_*: the learned hop proposal, new (the reference
  *                           samples with the uniform ParticleHop only); they extend the same
  *                           sampler call (code/states.py:397-408).
@@ -269,6 +271,19 @@ int nh_metropolis_steps(int8_t* spins, float* sign, double* logabs, int batch, i
                         const nh_backflow_params* p, int n_dirs, uint64_t seed, int64_t step0,
                         int nsteps, int32_t* accepted, void* workspace, size_t workspace_bytes,
                         void* stream);
+
+/* Mixed hop / site-exchange Metropolis (the reference's MixSampler of a ParticleHop and a
+ * SiteExchange sampler, code/states.py:397-408): chains b < first_exchange make the plain hop
+ * steps of nh_metropolis_steps; chains b >= first_exchange make site-exchange steps, in which a
+ * uniform site i and a uniform one of its n_dirs neighbours j swap their occupations (both spin
+ * species; equal occupations are a null move), so one step can move an up and a down electron.
+ * The proposal is symmetric and accepted with min(1, |psi(s')/psi(s)|^2).  Same random-number
+ * streams and buffers as nh_metropolis_steps (draw x -> site, y -> direction, z -> acceptance);
+ * nh_metropolis_steps is this call with first_exchange = batch. */
+int nh_metropolis_steps_mixed(int8_t* spins, float* sign, double* logabs, int batch, int n_symm,
+                              const nh_backflow_params* p, int n_dirs, int first_exchange,
+                              uint64_t seed, int64_t step0, int nsteps, int32_t* accepted,
+                              void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- Learned hop proposal ----
  * A periodic 3x3 CNN 2 -> 16 -> 16 -> 16 (tanh-GELU after layers 1 and 2) on the +-1 occupation

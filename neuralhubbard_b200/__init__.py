@@ -8,7 +8,8 @@ Drop-in surface (after ChenAo-Phys/NeuralHubbard's quantax usage):
     psi = state(spins)                                    # psi.sign, psi.logabs
     H = Hubbard(U=8.0, t=[1.0, -0.2], n_neighbor=[1, 2])  # code/states.py:244-247
     eloc = H.Oloc(state, Samples(spins, psi))             # code/quick_start.py:33
-    sampler = ParticleHop(state, 8192, n_neighbor=(1, 2)) # code/states.py:397-408
+    sampler = MixSampler([ParticleHop(state, 4096, n_neighbor=(1, 2)),  # code/states.py:397-408
+                          SiteExchange(state, 4096, n_neighbor=(1, 2))])
     samples = sampler.sweep()
 
 Learned proposal (new): HopProposal (network, GPU training), training_records (data from plain
@@ -19,7 +20,7 @@ from ._lib import NativeLibraryError
 from .backflow import PairGeometry, PfaffianBackflow, build_wtilde, init_params, pairing_occ, slogpf
 from .operator import Hubbard
 from .proposal import HopProposal, LearnedHop, training_records
-from .sampler import ParticleHop, random_spins
+from .sampler import MixSampler, ParticleHop, SiteExchange, random_spins
 from .state import LogArray, Samples, Variational
 
 __all__ = [
@@ -35,6 +36,8 @@ __all__ = [
     "LearnedHop",
     "training_records",
     "ParticleHop",
+    "SiteExchange",
+    "MixSampler",
     "random_spins",
     "LogArray",
     "Samples",

@@ -100,6 +100,9 @@ SIGNATURES = {
     "nh_metropolis_steps": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, P_BF, c_int,
                                     c_uint64, c_int64, c_int, c_void_p, c_void_p, c_size_t,
                                     c_void_p]),
+    "nh_metropolis_steps_mixed": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, P_BF,
+                                          c_int, c_int, c_uint64, c_int64, c_int, c_void_p,
+                                          c_void_p, c_size_t, c_void_p]),
     "nh_proposal_pack": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "nh_proposal_forward": (c_int, [c_void_p, c_int, P_Q, c_void_p, c_void_p]),
     "nh_proposal_sample": (c_int, [c_void_p, c_int, P_Q, c_uint64, c_int64, c_void_p, c_void_p,

@@ -615,11 +615,22 @@ int nh_metropolis_steps(int8_t* spins, float* sign, double* logabs, int batch, i
                         const nh_backflow_params* p, int n_dirs, uint64_t seed, int64_t step0,
                         int nsteps, int32_t* accepted, void* workspace, size_t workspace_bytes,
                         void* stream) {
+  return nh_metropolis_steps_mixed(spins, sign, logabs, batch, n_symm, p, n_dirs, batch, seed,
+                                   step0, nsteps, accepted, workspace, workspace_bytes, stream);
+}
+
+int nh_metropolis_steps_mixed(int8_t* spins, float* sign, double* logabs, int batch, int n_symm,
+                              const nh_backflow_params* p, int n_dirs, int first_exchange,
+                              uint64_t seed, int64_t step0, int nsteps, int32_t* accepted,
+                              void* workspace, size_t workspace_bytes, void* stream) {
   int rc = check_params(p);
   if (rc) return rc;
   if (n_dirs != 4 && n_dirs != 8) return fail(NH_ERR_INVALID, "metropolis: n_dirs %d", n_dirs);
   if (!spins || !sign || !logabs || batch < 0 || nsteps < 0)
     return fail(NH_ERR_INVALID, "metropolis: bad buffers");
+  if (first_exchange < 0 || first_exchange > batch)
+    return fail(NH_ERR_INVALID, "metropolis: first_exchange %d outside [0, %d]", first_exchange,
+                batch);
   if (n_symm != 1 && n_symm != 8) return fail(NH_ERR_INVALID, "metropolis: n_symm %d", n_symm);
   if (batch == 0 || nsteps == 0) return NH_OK;
   const size_t need = nh_metropolis_workspace_bytes(batch, n_symm, p);
@@ -631,7 +642,7 @@ int nh_metropolis_steps(int8_t* spins, float* sign, double* logabs, int batch, i
   for (int t = 0; t < nsteps; ++t) {
     const int64_t step = step0 + t;
     if ((rc = launch_mh_propose(spins, batch, p->Lx, p->Ly, n_dirs, seed, step, L.valid, L.from,
-                                L.to, st)))
+                                L.to, st, first_exchange)))
       return rc;
     if ((rc = launch_compact(L.valid, L.from, L.to, batch, L.c_sample, L.c_from, L.c_to,
                              L.c_count, st)))

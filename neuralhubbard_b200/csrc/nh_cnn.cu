@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
     for (int m = tid; m < M2; m += kNumThreads) {
       const int src = sym_map(m, g, a.Lx, a.Ly, N);  // image[m] = s[g(m)] (g is an involution)
       int v = base[src];
-      v = (src == fr) ? -1 : ((src == to) ? 1 : v);
+      v = move_value(src, v, fr, to);
       simg[m] = v > 0 ? 1 : -1;
       const int ch = m >= N ? 1 : 0;
       actA[ch * NS + (m - ch * N)] = v > 0 ? T(1) : T(-1);

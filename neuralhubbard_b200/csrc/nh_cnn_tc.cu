@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) cnn_tc_kernel(TcArgs a) {
     for (int m = ltid; m < M2; m += kWGThreads) {
       const int src = sym_map(m, g, kL, kL, N);
       int v = base[src];
-      v = (src == fr) ? -1 : ((src == to) ? 1 : v);
+      v = move_value(src, v, fr, to);
       simg[m] = v > 0 ? 1 : -1;
     }
     wg_sync(wg);

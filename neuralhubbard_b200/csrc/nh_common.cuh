@@ -178,6 +178,24 @@ __device__ void write_occupied_rows(const int* simg, int* occl, int* wbuf, int N
   }
 }
 
+// ------------------------------------------------------------------ moves
+// A move is one or two electron hops packed into (from, to): bits [0, 16) hold the first hop's
+// source and target modes, bits [16, 32) the second hop's modes plus one (0: no second hop).
+// A site exchange of an up and a down electron is two hops; every other move is one.  from = -1
+// (all bits set) matches no mode.
+__host__ __device__ __forceinline__ int pack_move(int m1, int m2) {
+  return (m1 & 0xFFFF) | (m2 >= 0 ? (m2 + 1) << 16 : 0);
+}
+__host__ __device__ __forceinline__ int move_first(int x) { return x & 0xFFFF; }
+__host__ __device__ __forceinline__ int move_second(int x) { return ((x >> 16) & 0xFFFF) - 1; }
+
+// Occupation of mode src after the move (from, to), v its value before.
+__host__ __device__ __forceinline__ int move_value(int src, int v, int from, int to) {
+  if (src == move_first(from) || src == move_second(from)) return -1;
+  if (src == move_first(to) || src == move_second(to)) return 1;
+  return v;
+}
+
 // ------------------------------------------------------------------ Philox4x32-10
 // Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC'11).
 struct u32x4 {
@@ -209,8 +227,8 @@ __host__ __device__ __forceinline__ double u32_to_unit(uint32_t x) {
 struct ConfigList {
   const int8_t* spins;       // (n_samples, 2N)
   const int32_t* sample;     // (n_cfg,) sample of each configuration, null: c itself
-  const int32_t* from;       // (n_cfg,) hop source mode or -1, null: no hop
-  const int32_t* to;         // (n_cfg,) hop target mode
+  const int32_t* from;       // (n_cfg,) packed move sources (pack_move) or -1, null: no move
+  const int32_t* to;         // (n_cfg,) packed move targets
   const int32_t* n_cfg_dev;  // device count (overrides n_cfg when not null)
   int n_cfg;                 // host count (upper bound when n_cfg_dev is set)
   int G;                     // images per configuration: 1 or 8
@@ -381,9 +399,11 @@ int launch_eloc_reduce(const int8_t* spins, const float* sign, const double* log
                        int N, double U, const int64_t* offsets, const double* hval,
                        const float* csign, const double* clogabs, double* eloc,
                        cudaStream_t st);
+// Chains b < first_exchange propose a uniform hop, chains b >= first_exchange a uniform site
+// exchange (a site and one of its n_dirs neighbours swap their occupations).
 int launch_mh_propose(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs,
                       uint64_t seed, int64_t step, int32_t* valid, int32_t* from, int32_t* to,
-                      cudaStream_t st);
+                      cudaStream_t st, int first_exchange = INT32_MAX);
 int launch_compact(const int32_t* valid, const int32_t* from, const int32_t* to, int batch,
                    int32_t* c_sample, int32_t* c_from, int32_t* c_to, int32_t* c_count,
                    cudaStream_t st);

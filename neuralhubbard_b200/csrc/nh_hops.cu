@@ -200,15 +200,47 @@ __global__ void eloc_reduce_kernel(const int8_t* __restrict__ spins, const float
 
 // One warp per chain: Philox draws (step, chain, 0, 0), electron of rank e = (r0 k) >> 32
 // among the k occupied modes (ascending), direction (r1 n_dirs) >> 32.
+// Site exchange (SiteExchange of code/states.py:397-408): a uniform site i and a uniform one of
+// its n_dirs neighbours j swap their occupations (up and down); equal occupations are a null
+// move.  Word 0 of the chain's draw picks the site, word 1 the direction (the reverse move picks
+// j and the opposite direction with the same probability: the proposal is symmetric).
+__device__ __forceinline__ void propose_exchange(const int8_t* s, int N, int Lx, int Ly,
+                                                 int n_dirs, u32x4 r, int32_t* valid,
+                                                 int32_t* from, int32_t* to) {
+  const int i = (int)(((uint64_t)r.x * (uint64_t)N) >> 32);
+  const int dir = (int)(((uint64_t)r.y * (uint64_t)n_dirs) >> 32);
+  const int j = hop_target_site(i, dir, Lx, Ly);
+  int src[2] = {-1, -1}, dst[2] = {-1, -1}, h = 0;
+  for (int sg = 0; sg < 2; ++sg) {
+    const bool oi = s[sg * N + i] > 0, oj = s[sg * N + j] > 0;
+    if (oi != oj) {
+      src[h] = sg * N + (oi ? i : j);
+      dst[h] = sg * N + (oi ? j : i);
+      ++h;
+    }
+  }
+  *valid = h > 0 ? 1 : 0;
+  *from = h > 0 ? pack_move(src[0], src[1]) : -1;
+  *to = h > 0 ? pack_move(dst[0], dst[1]) : -1;
+}
+
 __global__ void mh_propose_kernel(const int8_t* __restrict__ spins, int batch, int Lx, int Ly,
                                   int n_dirs, uint32_t k0, uint32_t k1, uint32_t step_lo,
-                                  uint32_t step_hi, int32_t* valid, int32_t* from, int32_t* to) {
+                                  uint32_t step_hi, int32_t* valid, int32_t* from, int32_t* to,
+                                  int first_exchange) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int N = Lx * Ly, M2 = 2 * N;
   for (int b = warp; b < batch; b += nwarps) {
     const int8_t* s = spins + (size_t)b * M2;
+    if (b >= first_exchange) {
+      if (lane == 0) {
+        const u32x4 r = philox4x32_10(u32x4{step_lo, (uint32_t)b, 0u, step_hi}, k0, k1);
+        propose_exchange(s, N, Lx, Ly, n_dirs, r, valid + b, from + b, to + b);
+      }
+      continue;
+    }
     int k = 0;
     for (int m = lane; m < M2; m += 32) k += s[m] > 0;
 #pragma unroll
@@ -299,8 +331,13 @@ __global__ void mh_accept_kernel(int8_t* spins, float* sign, double* logabs, int
     const bool acc = sp != 0.0f && (u == 0.0 || log(u) < lr2);
     if (acc) {
       int8_t* s = spins + (size_t)b * 2 * N;
-      s[c_from[i]] = -1;
-      s[c_to[i]] = 1;
+      const int f = c_from[i], t = c_to[i];
+      s[move_first(f)] = -1;
+      s[move_first(t)] = 1;
+      if (move_second(f) >= 0) {
+        s[move_second(f)] = -1;
+        s[move_second(t)] = 1;
+      }
       sign[b] = sp;
       logabs[b] = plogabs[i];
       if (accepted) accepted[b] += 1;
@@ -427,13 +464,14 @@ int launch_eloc_reduce(const int8_t* spins, const float* sign, const double* log
 
 int launch_mh_propose(const int8_t* spins, int batch, int Lx, int Ly, int n_dirs,
                       uint64_t seed, int64_t step, int32_t* valid, int32_t* from, int32_t* to,
-                      cudaStream_t st) {
+                      cudaStream_t st, int first_exchange) {
   if (batch <= 0) return NH_OK;
   int grid = min((batch + 7) / 8, num_sms() * 16);
   ProfScope prof_scope(NH_K_MH_PROPOSE, st);
   mh_propose_kernel<<<grid, 256, 0, st>>>(spins, batch, Lx, Ly, n_dirs, (uint32_t)seed,
                                           (uint32_t)(seed >> 32), (uint32_t)step,
-                                          (uint32_t)((uint64_t)step >> 32), valid, from, to);
+                                          (uint32_t)((uint64_t)step >> 32), valid, from, to,
+                                          first_exchange);
   return check_launch("mh_propose_kernel");
 }
 

@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(kRcThreads, 1) resconv_kernel(RcArgs<T> a) {
     for (int m = tid; m < M2; m += kRcThreads) {
       const int src = sym_map(m, g, a.Lx, a.Ly, N);  // image[m] = s[g(m)] (g is an involution)
       int v = base[src];
-      v = (src == fr) ? -1 : ((src == to) ? 1 : v);
+      v = move_value(src, v, fr, to);
       simg[m] = v > 0 ? 1 : -1;
     }
     __syncthreads();

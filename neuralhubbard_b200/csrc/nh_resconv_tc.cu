@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(kRtThreads, 1) resconv_tc_kernel(RtArgs a) {
     for (int m = tid; m < 2 * kRtN; m += kRtThreads) {
       const int src = sym_map(m, g, kL, kL, kRtN);
       int v = base[src];
-      v = (src == fr) ? -1 : ((src == to) ? 1 : v);
+      v = move_value(src, v, fr, to);
       simg[m] = v > 0 ? 1 : -1;
     }
     __syncthreads();

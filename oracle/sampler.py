@@ -9,6 +9,14 @@ occupied mode uniformly (rank e among the k occupied modes, ascending), pick one
 ``n_dirs`` hop directions uniformly; if the target mode of the same spin is empty the move
 is proposed, otherwise the step is a null move.  The proposal is symmetric, so a move is
 accepted when u < |psi(s') / psi(s)|^2.
+
+Site exchange (the SiteExchange analogue of ``code/states.py:397-408``): pick a site i
+uniformly (word 0 of the draw) and one of the ``n_dirs`` directions (word 1); the site j it
+reaches swaps its occupation (up and down) with i.  Equal occupations are a null move; an up and
+a down electron may move in one step.  The reverse move (j and the opposite direction) has the
+same probability, so the proposal is symmetric.  The mixed sampler (``MixSampler`` of a
+ParticleHop and a SiteExchange sampler) runs hops on chains b < first_exchange and exchanges on
+the others.
 """
 
 from __future__ import annotations
@@ -72,6 +80,26 @@ def propose_uniform(s: np.ndarray, r0, r1, Lx: int, Ly: int, n_dirs: int = 8):
     return fr, to, ok
 
 
+def propose_exchange(s: np.ndarray, r0, r1, Lx: int, Ly: int, n_dirs: int = 8):
+    """Site-exchange proposal for each chain: a list of (from_mode, to_mode) hops (0, 1 or 2)
+    and valid (at least one hop)."""
+    N = Lx * Ly
+    nbr = lattice.neighbour_table(Lx, Ly)
+    moves, ok = [], np.zeros(s.shape[0], bool)
+    for b in range(s.shape[0]):
+        i = (int(r0[b]) * N) >> 32
+        j = int(nbr[i, (int(r1[b]) * n_dirs) >> 32])
+        hops = []
+        for sigma in range(2):
+            oi, oj = s[b, sigma * N + i] > 0, s[b, sigma * N + j] > 0
+            if oi != oj:
+                src, dst = (i, j) if oi else (j, i)
+                hops.append((sigma * N + src, sigma * N + dst))
+        moves.append(hops)
+        ok[b] = len(hops) > 0
+    return moves, ok
+
+
 def metropolis_accept(log_ratio2: np.ndarray, r2) -> np.ndarray:
     """Accept when u < exp(log_ratio2), compared as log(u) < log_ratio2 (FP64)."""
     u = uniform_from_u32(r2)
@@ -79,22 +107,33 @@ def metropolis_accept(log_ratio2: np.ndarray, r2) -> np.ndarray:
         return np.log(u) < log_ratio2
 
 
-def metropolis_steps(s, psi, amp_fn, Lx, Ly, seed, step0, nsteps, n_dirs=8):
-    """Run ``nsteps`` plain Metropolis steps on every chain.  Returns (s, sign, logabs,
-    accepted count per chain)."""
+def metropolis_steps(s, psi, amp_fn, Lx, Ly, seed, step0, nsteps, n_dirs=8,
+                     first_exchange=None):
+    """Run ``nsteps`` Metropolis steps on every chain: hops on chains b < first_exchange (all
+    chains when None), site exchanges on the others.  Returns (s, sign, logabs, accepted count
+    per chain)."""
     s = np.array(s, copy=True)
     sign, logabs = (np.array(a, dtype=np.float64, copy=True) for a in psi)
-    chains = np.arange(s.shape[0])
-    acc = np.zeros(s.shape[0], np.int64)
+    B = s.shape[0]
+    fx = B if first_exchange is None else int(first_exchange)
+    chains = np.arange(B)
+    acc = np.zeros(B, np.int64)
     for t in range(step0, step0 + nsteps):
         r = draws(seed, t, chains)
         fr, to, ok = propose_uniform(s, r[0], r[1], Lx, Ly, n_dirs)
+        moves = [[(int(fr[b]), int(to[b]))] for b in range(B)]
+        if fx < B:
+            mx, okx = propose_exchange(s[fx:], r[0][fx:], r[1][fx:], Lx, Ly, n_dirs)
+            moves[fx:] = mx
+            ok[fx:] = okx
         idx = np.flatnonzero(ok)
         if len(idx) == 0:
             continue
         sp = s[idx].copy()
-        sp[np.arange(len(idx)), fr[idx]] = -1
-        sp[np.arange(len(idx)), to[idx]] = 1
+        for k, b in enumerate(idx):
+            for m_from, m_to in moves[b]:
+                sp[k, m_from] = -1
+                sp[k, m_to] = 1
         sg2, la2 = amp_fn(sp)
         a = metropolis_accept(2.0 * (la2 - logabs[idx]), r[2][idx]) & (sg2 != 0)
         sel = idx[a]

@@ -265,6 +265,7 @@ def test_unfused_path_is_bitwise_equal():
     F = nh.pairing_occ(Y.contiguous(), idx, model.Wt, g)
     sg, la, _ = nh.slogpf(F, cond_tau=0.0)
     model.cond_tau = 0.0
+    model.refine_tau = 0.0
     psi = nh.Variational(model, symm=False)(ts)
     assert torch.equal(psi.sign, sg) and torch.equal(psi.logabs, la)
 
@@ -371,6 +372,37 @@ def test_metropolis_bookkeeping_replay():
     assert np.array_equal(smp.accepted.cpu().numpy(), acc)
     assert np.array_equal(smp.psi.logabs.cpu().numpy(), la_ref)
     # particle numbers conserved
+    assert np.all((s_gpu[:, : g.N] > 0).sum(1) == g.n_up)
+    assert np.all((s_gpu[:, g.N :] > 0).sum(1) == g.n_dn)
+
+
+def test_mixed_sampler_bookkeeping_replay():
+    """MixSampler([ParticleHop, SiteExchange]) (code/states.py:397-408): hop steps on the first
+    half of the chains, site exchanges on the second; the chains equal an oracle replay with the
+    same Philox draws and the GPU amplitudes of the proposed configurations, bit for bit."""
+    L = 8
+    model = make_model(L, std=0.3, seed=5)
+    g = model.geom
+    state = nh.Variational(model, symm=False)
+    s0 = olat.random_configs(np.random.default_rng(17), 48, g.N, g.n_up, g.n_dn)
+    hop = nh.ParticleHop(state, 24, n_neighbor=(1, 2))
+    exc = nh.SiteExchange(state, 24, n_neighbor=(1, 2))
+    smp = nh.MixSampler([hop, exc], initial_spins=s0, seed=4321)
+    assert smp.first_exchange == 24 and smp.nsamples == 48
+    psi0 = (smp.psi.sign.cpu().numpy().astype(np.float64), smp.psi.logabs.cpu().numpy())
+    smp.run(30)
+    s_gpu = smp.spins.cpu().numpy()
+
+    def amp(c):
+        sg, la = state(c).numpy()
+        return sg.astype(np.float64), la
+
+    s_ref, sg_ref, la_ref, acc = osam.metropolis_steps(s0, psi0, amp, L, L, 4321, 0, 30,
+                                                       first_exchange=24)
+    assert np.array_equal(s_gpu, s_ref)
+    assert np.array_equal(smp.accepted.cpu().numpy(), acc)
+    assert np.array_equal(smp.psi.logabs.cpu().numpy(), la_ref)
+    assert acc[24:].sum() > 0  # exchanges were accepted
     assert np.all((s_gpu[:, : g.N] > 0).sum(1) == g.n_up)
     assert np.all((s_gpu[:, g.N :] > 0).sum(1) == g.n_dn)
 
