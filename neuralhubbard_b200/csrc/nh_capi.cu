@@ -114,7 +114,7 @@ size_t pipeline_bytes(int max_items, const nh_backflow_params& p) {
          align256(it * sizeof(int32_t)) * 2 + align256(sizeof(int32_t)) +
          align256(it * n * d * sizeof(double)) + align256(it * n * sizeof(int32_t)) +
          align256(sizeof(int32_t)) + align256(pfaffian_scratch_bytes((int)n)) +
-         align256(act_scratch_bytes(p)) + refine_bytes(it, (int)n);
+         align256(act_scratch_bytes(p)) + align256(it * sizeof(float)) + refine_bytes(it, (int)n);
 }
 
 PipelineBuffers carve_pipeline(void* ws, int max_items, const nh_backflow_params& prm) {
@@ -141,6 +141,7 @@ PipelineBuffers carve_pipeline(void* ws, int max_items, const nh_backflow_params
   const size_t tri_bytes = pfaffian_scratch_bytes((int)n), act_bytes = act_scratch_bytes(prm);
   b.pf_tri = tri_bytes ? take(tri_bytes) : nullptr;
   b.cnn_act = act_bytes ? take(act_bytes) : nullptr;
+  b.pf_ratio = reinterpret_cast<float*>(take(it * sizeof(float)));
   b.perm = nullptr;
   b.list32 = b.count32 = nullptr;
   b.slice = nullptr;
@@ -180,6 +181,7 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
   const bool refine = b.perm != nullptr;  // n <= kRefineMaxN
   PfGatherArgs g{b.Y, b.idx, p.Wt, p.Lx, p.Ly, d, n, cl.n_cfg_dev, cl.G, max_items, nullptr,
                  b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, p.cond_tau, 0, false, b.pf_tri};
+  g.ratio = b.pf_ratio;
   if (refine) {
     g.perm = b.perm;
     g.refine_tau = p.refine_tau;
@@ -189,9 +191,9 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
     return rc;
   const bool fp64 = p.Wt64 && (p.cond_tau > 0.0 || (p.cancel_tau > 0.0 && cl.G > 1));
   if (fp64) {
-    // cond_tau <= 1 flags every image (the all-FP64 form): nothing is pruned then.
-    if ((rc = launch_image_mark(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev,
-                                p.cancel_tau, p.cond_tau > 1.0, st)))
+    // cond_tau <= 1 flags every image (the all-FP64 form): no weighting then.
+    if ((rc = launch_image_mark(b.pf_sign, b.pf_logabs, b.pf_flags, b.pf_ratio, cl.G, cl.n_cfg,
+                                cl.n_cfg_dev, p.cancel_tau, p.cond_tau, p.cond_tau > 1.0, st)))
       return rc;
     if ((rc = launch_flagged(b.pf_flags, max_items, cl.n_cfg_dev, cl.G, b.list, b.count, st)))
       return rc;

@@ -248,6 +248,7 @@ struct PipelineBuffers {
   int32_t* err;       // (1,) device error word of the tensor-core CNN
   void* pf_tri;       // large lattices: per-CTA Pfaffian triangles (pfaffian_scratch_bytes)
   void* cnn_act;      // large lattices: per-CTA CNN activation planes (cnn_scratch_bytes)
+  float* pf_ratio;    // (items,) pivot ratio of the FP32 factorisation
   uint16_t* perm;     // (items, perm_stride) FP32 pivot order of every item (n <= kRefineMaxN)
   int32_t* list32;    // (items,) items refined against their FP32 matrix
   int32_t* count32;   // (1,) their number
@@ -319,6 +320,7 @@ struct PfGatherArgs {
   void* tri;  // per-CTA triangles for n beyond shared memory (pfaffian_scratch_bytes), or null
   uint16_t* perm = nullptr;  // when set: the pivot order of every item (perm_stride(n) words)
   double refine_tau = 0.0;   // pivot ratio above which kFlagNeedRefine is set (0: never)
+  float* ratio = nullptr;    // when set: every item's pivot ratio
 };
 
 // Launchers (return NH_OK or an error code).
@@ -343,10 +345,12 @@ int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, 
                    const int32_t* n_cfg_dev, float* sign, double* logabs, int32_t* flags,
                    double cancel_tau, const int32_t* err, cudaStream_t st);
 // Projected amplitudes (G > 1): marks every image of a configuration whose images cancel
-// (sum |.| > cancel_tau |sum|) with NH_FLAG_GROWTH | NH_FLAG_CANCEL, and unmarks ill-conditioned
-// images too small to matter, before the FP64 recompute list is built.
-int launch_image_mark(const float* sg, const double* la, int32_t* fl, int G, int n_cfg,
-                      const int32_t* n_cfg_dev, double cancel_tau, bool prune, cudaStream_t st);
+// (sum |.| > cancel_tau |sum|) with NH_FLAG_GROWTH | NH_FLAG_CANCEL and, with weighted, marks
+// exactly the other images whose share of psi_P times pivot ratio exceeds cond_tau, before the
+// FP64 recompute list is built.
+int launch_image_mark(const float* sg, const double* la, int32_t* fl, const float* ratio, int G,
+                      int n_cfg, const int32_t* n_cfg_dev, double cancel_tau, double cond_tau,
+                      bool weighted, cudaStream_t st);
 // Ordered list of the items whose flags have a bit of set_mask and none of clear_mask.
 int launch_flagged(const int32_t* flags, int n_items, const int32_t* count_dev, int count_mult,
                    int32_t* list, int32_t* count, cudaStream_t st, int set_mask = NH_FLAG_GROWTH,

@@ -89,6 +89,7 @@ struct PfArgs {
   void* tri;                 // large n: per-CTA lower triangles of T in global memory
   uint16_t* perm;            // or null: per item, logical -> physical row, then the parity
   double refine_tau;         // set kFlagNeedRefine when max|piv| > refine_tau min|piv| (0: off)
+  float* ratio;              // or null: per item, max|piv| / min|piv| (inf for a zero pivot)
 };
 
 __device__ __forceinline__ int tri_off(int i) { return (i * (i - 1)) >> 1; }
@@ -411,7 +412,7 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
       // Pfaffian = relabelling parity x product of the pivots, accumulated in FP64 as mantissa
       // and exponent; the pivot ratio flags near-nodal blocks.
       float s = a.item_sign ? a.item_sign[item] : 1.0f;
-      double la;
+      double la, pmax_all = 0.0, pmin_all = 1.0;
       if (isnan(s)) flag |= NH_FLAG_NONFINITE;  // the CNN could not compute this item
       if (zero) {
         s = 0.0f;
@@ -436,11 +437,14 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
         if (!isfinite(la)) flag |= NH_FLAG_NONFINITE;
         if (a.cond_tau > 0.0 && pmax > a.cond_tau * pmin) flag |= NH_FLAG_GROWTH;
         if (a.refine_tau > 0.0 && pmax > a.refine_tau * pmin) flag |= kFlagNeedRefine;
+        pmax_all = pmax;
+        pmin_all = pmin;
       }
       if (s == 0.0f) la = -INFINITY;
       a.sign[item] = s;
       a.logabs[item] = la;
       if (a.flags) a.flags[item] = flag | a.flag_or;
+      if (a.ratio) a.ratio[item] = zero ? INFINITY : (float)(pmax_all / pmin_all);
     }
     // Pivot order for the FP64 refinement: every row's final logical label, and the parity.
     if (a.perm && !zero) {
@@ -673,18 +677,21 @@ __device__ __forceinline__ double image_sum(const float* __restrict__ sg,
   return tot;
 }
 
-// Recompute selection for projected amplitudes, before the FP64 list is built.  An image's
-// error reaches log|psi_P| weighted by w_g = |psi_g| / |sum_g eta_g psi_g|.  In a configuration
-// whose images cancel (sum |.| > cancel_tau |sum|, cancel_tau > 0) the images with
-// w_g > kCancelImageFloor are marked: an FP32 image error (at most ~1e-3) of the others adds
-// < 2e-5.  An ill-conditioned image (NH_FLAG_GROWTH) with w_g < kImageWeightFloor is unmarked:
-// even a 1e-2 error in it moves log|psi_P| by < 1e-5.
-constexpr double kImageWeightFloor = 1e-3;
+// FP64-feature selection for projected amplitudes, before the FP64 list is built.  An image's
+// error reaches log|psi_P| weighted by its share w_g = eta_g psi_g / psi_P (sum_g w_g = 1,
+// sum_g |w_g| = C), and the error of an image with FP32 (or BF16x3) features grows with its
+// pivot ratio r_g.  In a configuration whose images cancel (C > cancel_tau > 0) every image
+// with |w_g| > kCancelImageFloor is marked (NH_FLAG_GROWTH | NH_FLAG_CANCEL): an FP32 image
+// error (at most ~1e-3) of the others adds < 2e-5.  Otherwise, with weighted set, an image is
+// marked exactly when |w_g| r_g > cond_tau (its estimated error, up to the features' relative
+// accuracy), and unmarked when not; without weighted (cond_tau <= 1, every image already
+// marked) the marks stay.
 constexpr double kCancelImageFloor = 2e-2;
 
 __global__ void image_mark_kernel(const float* __restrict__ sg, const double* __restrict__ la,
-                                  int32_t* __restrict__ fl, int G, int n_cfg,
-                                  const int32_t* n_cfg_dev, double cancel_tau, bool prune) {
+                                  int32_t* __restrict__ fl, const float* __restrict__ ratio,
+                                  int G, int n_cfg, const int32_t* n_cfg_dev, double cancel_tau,
+                                  double cond_tau, bool weighted) {
   const int n = n_cfg_dev ? *n_cfg_dev : n_cfg;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
     double m, a;
@@ -695,13 +702,13 @@ __global__ void image_mark_kernel(const float* __restrict__ sg, const double* __
         if (sg[i] != 0.0f && exp(la[i] - m) > kCancelImageFloor * fabs(tot))
           fl[i] |= NH_FLAG_GROWTH | NH_FLAG_CANCEL;
       }
-    } else if (prune && tot != 0.0) {
+    } else if (weighted && tot != 0.0) {
       for (int g = 0; g < G; ++g) {
         const size_t i = (size_t)c * G + g;
         const int f = fl[i];
-        if ((f & NH_FLAG_GROWTH) && !(f & NH_FLAG_NONFINITE) && sg[i] != 0.0f &&
-            exp(la[i] - m) < kImageWeightFloor * fabs(tot))
-          fl[i] = f & ~NH_FLAG_GROWTH;
+        if ((f & (NH_FLAG_NONFINITE | NH_FLAG_ZERO_PIVOT)) || sg[i] == 0.0f) continue;
+        const double w = exp(la[i] - m) / fabs(tot);
+        fl[i] = w * (double)ratio[i] > cond_tau ? (f | NH_FLAG_GROWTH) : (f & ~NH_FLAG_GROWTH);
       }
     }
   }
@@ -1080,7 +1087,7 @@ __global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, i
     }
     if (tid == 0) {
       float s = a.item_sign ? a.item_sign[item] : 1.0f;
-      double la;
+      double la, pmax_all = 0.0, pmin_all = 1.0;
       if (isnan(s)) flag |= NH_FLAG_NONFINITE;
       if (abort) {
         s = NAN;
@@ -1109,11 +1116,14 @@ __global__ void __launch_bounds__(kNumThreads, 1) pfaffian_tc_kernel(PfArgs a, i
         if (!isfinite(la)) flag |= NH_FLAG_NONFINITE;
         if (a.cond_tau > 0.0 && pmax > a.cond_tau * pmin) flag |= NH_FLAG_GROWTH;
         if (a.refine_tau > 0.0 && pmax > a.refine_tau * pmin) flag |= kFlagNeedRefine;
+        pmax_all = pmax;
+        pmin_all = pmin;
       }
       if (s == 0.0f) la = -INFINITY;
       a.sign[item] = s;
       a.logabs[item] = la;
       if (a.flags) a.flags[item] = flag | a.flag_or;
+      if (a.ratio) a.ratio[item] = (zero || abort) ? INFINITY : (float)(pmax_all / pmin_all);
     }
     if (a.perm && !zero && !abort) {
       uint16_t* pr = a.perm + (size_t)item * perm_stride(n);
@@ -1216,6 +1226,7 @@ int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st) {
   a.tri = g.tri;
   a.perm = g.perm;
   a.refine_tau = g.refine_tau;
+  a.ratio = g.ratio;
   return g.fp64 ? launch_pf_d<double>(a, g.d, st) : launch_pf_d<float>(a, g.d, st);
 }
 
@@ -1245,6 +1256,7 @@ int launch_pfaffian_tc(const PfGatherArgs& g, int mode, const float* F, int32_t*
   a.flag_or = g.flag_or;
   a.perm = g.perm;
   a.refine_tau = g.refine_tau;
+  a.ratio = g.ratio;
   switch (mode == 0 ? 16 : g.d) {
     case 8: return launch_pf_tc<8>(a, err, st);
     case 16: return launch_pf_tc<16>(a, err, st);
@@ -1305,12 +1317,15 @@ int launch_combine(const float* sg, const double* la, const int32_t* fl, int G, 
   return check_launch("combine_kernel");
 }
 
-int launch_image_mark(const float* sg, const double* la, int32_t* fl, int G, int n_cfg,
-                      const int32_t* n_cfg_dev, double cancel_tau, bool prune, cudaStream_t st) {
-  if (n_cfg <= 0 || G <= 1 || (cancel_tau <= 0.0 && !prune)) return NH_OK;
+int launch_image_mark(const float* sg, const double* la, int32_t* fl, const float* ratio, int G,
+                      int n_cfg, const int32_t* n_cfg_dev, double cancel_tau, double cond_tau,
+                      bool weighted, cudaStream_t st) {
+  weighted = weighted && ratio;
+  if (n_cfg <= 0 || G <= 1 || (cancel_tau <= 0.0 && !weighted)) return NH_OK;
   int grid = (n_cfg + 255) / 256;
   ProfScope prof_scope(NH_K_COMBINE, st);
-  image_mark_kernel<<<grid, 256, 0, st>>>(sg, la, fl, G, n_cfg, n_cfg_dev, cancel_tau, prune);
+  image_mark_kernel<<<grid, 256, 0, st>>>(sg, la, fl, ratio, G, n_cfg, n_cfg_dev, cancel_tau,
+                                          cond_tau, weighted);
   return check_launch("image_mark_kernel");
 }
 

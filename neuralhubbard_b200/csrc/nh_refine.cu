@@ -17,7 +17,7 @@
 // F[p, q] = sum_a (Y[p, a] Y[q, a]) Wt[2 s_p + s_q, r(p, q), a], in the same order of operations
 // as the FP32 gather so that the FP32 matrix is reproduced bit for bit.
 //
-// One CTA (512 threads) per SM.  Phase 1 stages the Wt table and the item's features in shared
+// One CTA (256 threads) per SM.  Phase 1 stages the Wt table and the item's features in shared
 // memory and writes the permuted lower triangle to a per-CTA slice of global scratch (L2
 // resident); phase 2 loads it into shared memory as FP64 (row a at roff(a), rows 16-byte
 // aligned); phase 3 eliminates.  n <= kRefineMaxN (224: the FP64 triangle takes 200 KB).
@@ -30,7 +30,7 @@
 namespace nh {
 namespace {
 
-constexpr int kRThreads = 512;
+constexpr int kRThreads = 256;
 constexpr int kRWarps = kRThreads / 32;
 constexpr int kPW = 8;  // panel width: 4 elimination steps
 
@@ -89,20 +89,35 @@ __device__ void gather_permuted(const RefineArgs& a, int item, int slot, const i
   T* ys = reinterpret_cast<T*>(smem);                    // (n, DP)
   int* info = reinterpret_cast<int*>(ys + n * DP);       // (n) spin << 16 | x << 8 | y
   T* wts = reinterpret_cast<T*>(info + ((n + 3) & ~3));  // (4 N, DP) when staged
-  for (int e = tid; e < n * D; e += kRThreads) {
-    const int r = e / D;
-    ys[r * DP + (e - r * D)] = Yg[e];
-  }
+  // Row r of the source (D values, 16-byte vectors) to row r of the padded staging copy; several
+  // vectors in flight per thread.
+  auto stage = [&](const T* src, T* dst, int rows) {
+    constexpr int VPR = D / VK;  // vectors per row
+    const int nv = rows * VPR;
+    for (int v0 = tid; v0 < nv; v0 += 4 * kRThreads) {
+      V buf[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int v = v0 + u * kRThreads;
+        if (v < nv) buf[u] = __ldg(reinterpret_cast<const V*>(src) + v);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int v = v0 + u * kRThreads;
+        if (v < nv) {
+          const int r = v / VPR;
+          *reinterpret_cast<V*>(dst + r * DP + (v - r * VPR) * VK) = buf[u];
+        }
+      }
+    }
+  };
+  stage(Yg, ys, n);
   for (int p = tid; p < n; p += kRThreads) {
     const int m = ig[p];
     const int sp = m >= N ? 1 : 0, site = m - sp * N, x = site / a.Ly;
     info[p] = (sp << 16) | (x << 8) | (site - x * a.Ly);
   }
-  if (a.stage_wt)
-    for (int e = tid; e < 4 * N * D; e += kRThreads) {
-      const int r = e / D;
-      wts[r * DP + (e - r * D)] = Wg[e];
-    }
+  if (a.stage_wt) stage(Wg, wts, 4 * N);
   __syncthreads();
   int total = 0;
   for (int qb = 0; 32 * qb + 1 < n; ++qb) total += n - 32 * qb - 1;
@@ -163,12 +178,46 @@ __device__ void gather_permuted(const RefineArgs& a, int item, int slot, const i
   }
 }
 
+// The CTA's slice (tot values, tot a multiple of 4) into the FP64 triangle, 16-byte vectors with
+// four in flight per thread.
+__device__ __forceinline__ void copy_slice(const float* sl, double* S, int tot) {
+  const int nv = tot / 4;
+  for (int v0 = threadIdx.x; v0 < nv; v0 += 4 * kRThreads) {
+    float4 buf[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (v0 + u * kRThreads < nv) buf[u] = reinterpret_cast<const float4*>(sl)[v0 + u * kRThreads];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int v = v0 + u * kRThreads;
+      if (v < nv) {
+        reinterpret_cast<double2*>(S)[2 * v] = make_double2(buf[u].x, buf[u].y);
+        reinterpret_cast<double2*>(S)[2 * v + 1] = make_double2(buf[u].z, buf[u].w);
+      }
+    }
+  }
+}
+__device__ __forceinline__ void copy_slice(const double* sl, double* S, int tot) {
+  const int nv = tot / 2;
+  for (int v0 = threadIdx.x; v0 < nv; v0 += 4 * kRThreads) {
+    double2 buf[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (v0 + u * kRThreads < nv) buf[u] = reinterpret_cast<const double2*>(sl)[v0 + u * kRThreads];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (v0 + u * kRThreads < nv) reinterpret_cast<double2*>(S)[v0 + u * kRThreads] = buf[u];
+  }
+}
+
 template <int D>
 __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int perm_s[kRefineMaxN];
   __shared__ double Lm[kPW * kPW];  // block multipliers L[r][c] of the current panel
   __shared__ double xs[kPW / 2];    // its FP64 pivots
+  __shared__ double xinv[kPW / 2];  // and their reciprocals
+  __shared__ double xy[2][kPW];     // pivot-block columns k, k+1 of the current step
   const int n = a.n;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   double* S = reinterpret_cast<double*>(smem);
@@ -196,12 +245,12 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
         float* sl = reinterpret_cast<float*>(a.slice) + (size_t)blockIdx.x * tot;
         gather_permuted<float, D>(a, item, slot, perm_s, smem, sl);
         __syncthreads();  // slice written; the staging area is dead
-        for (int e = tid; e < tot; e += kRThreads) S[e] = (double)sl[e];
+        copy_slice(sl, S, tot);
       } else {
         double* sl = a.slice + (size_t)blockIdx.x * tot;
         gather_permuted<double, D>(a, item, slot, perm_s, smem, sl);
         __syncthreads();
-        for (int e = tid; e < tot; e += kRThreads) S[e] = sl[e];
+        copy_slice(sl, S, tot);
       }
     }
     __syncthreads();
@@ -212,7 +261,8 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
     for (int k0 = 0; k0 < n; k0 += kPW) {
       const int w = min(kPW, n - k0), steps = w >> 1;
       if (wid == 0) {
-        // (1) factorise the w x w pivot block: lane r holds row r, row[c] = B[r][c] (c < r).
+        // (1) factorise the w x w pivot block: lane r holds row r, row[c] = B[r][c] (c < r);
+        // each step's columns k, k+1 go through shared memory to every lane.
         double row[kPW];
 #pragma unroll
         for (int c = 0; c < kPW; ++c)
@@ -222,19 +272,26 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
           if (t < steps) {
             const int k = 2 * t;
             const double xr = row[k], yr = row[k + 1];  // B[r][k], B[r][k+1] (lanes r > k+1)
-            const double piv = -__shfl_sync(0xffffffffu, row[k], k + 1);  // B[k][k+1]
+            if (lane < kPW) {
+              xy[0][lane] = xr;
+              xy[1][lane] = yr;
+            }
+            __syncwarp();
+            const double piv = -xy[0][k + 1];  // B[k][k+1] = -B[k+1][k]
             const double inv = 1.0 / piv;
-            if (lane == 0) xs[t] = piv;
+            if (lane == 0) {
+              xs[t] = piv;
+              xinv[t] = inv;
+            }
             if (lane >= k + 2 && lane < w) {
               Lm[lane * kPW + k] = yr * inv;
               Lm[lane * kPW + k + 1] = -xr * inv;
             }
+            const double yi = yr * inv, xi = xr * inv;
 #pragma unroll
-            for (int c = 0; c < kPW; ++c) {
-              const double xc = __shfl_sync(0xffffffffu, xr, c);
-              const double yc = __shfl_sync(0xffffffffu, yr, c);
-              if (c >= k + 2 && c < lane && lane < w) row[c] += (yr * xc - xr * yc) * inv;
-            }
+            for (int c = 0; c < kPW; ++c)
+              if (c >= k + 2 && c < lane && lane < w) row[c] += yi * xy[0][c] - xi * xy[1][c];
+            __syncwarp();
           }
         }
       }
@@ -278,29 +335,32 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
 #pragma unroll
         for (int t = 0; t < kPW / 2; ++t) {
           if (2 * t < w) {
-            const double inv = 1.0 / xs[t];
+            const double inv = xinv[t];
             *reinterpret_cast<double2*>(sc + 2 * t) =
                 make_double2(wv[2 * t + 1] * inv, -wv[2 * t] * inv);
           }
         }
       }
       __syncthreads();
-      // (3) trailing update S[a][b] += sum_i P[a][i] W[i][b] for base <= b < a: warp <-> row a,
-      // lane <-> columns b0 = base + 64 cb + lane and b0 + 32 (their W in registers), the row's
-      // P broadcast.  All loads of a unit precede its stores.
+      // (3) trailing update S[a][b] += sum_i P[a][i] W[i][b] for base <= b < a: warp <-> a pair of
+      // rows, lane <-> columns b0 = base + 64 cb + lane and b0 + 32 (their W in registers), the
+      // rows' P broadcast; four elements and two partial sums each per lane keep the FP64 pipe
+      // fed.  All loads of a unit precede its stores.
       if (m >= 2) {
         double xv[kPW / 2];
 #pragma unroll
         for (int t = 0; t < kPW / 2; ++t) xv[t] = t < steps ? xs[t] : 0.0;
+        // units: (column block cb, row pair) over rows base + 64 cb + 1 .. n - 1
+        auto pairs = [&](int cb) { return (m - 64 * cb - 1 + 1) >> 1; };
         int total = 0;
-        for (int cb = 0; 64 * cb + 1 < m; ++cb) total += m - 64 * cb - 1;
+        for (int cb = 0; 64 * cb + 1 < m; ++cb) total += pairs(cb);
         int cb = 0, rem = wid, cur = -1;
         double w0[kPW], w1[kPW];
         int b0 = 0, b1 = 0;
 #pragma unroll 1
         for (int u = wid; u < total; u += kRWarps, rem += kRWarps) {
-          while (rem >= m - 64 * cb - 1) {
-            rem -= m - 64 * cb - 1;
+          while (rem >= pairs(cb)) {
+            rem -= pairs(cb);
             ++cb;
           }
           if (cb != cur) {
@@ -310,8 +370,8 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
 #pragma unroll
             for (int t = 0; t < kPW / 2; ++t) {
               double2 p0 = make_double2(0.0, 0.0), p1 = make_double2(0.0, 0.0);
-              if (2 * t < w && b0 < n) p0 = *reinterpret_cast<const double2*>(S + roff(b0) + k0 + 2 * t);
-              if (2 * t < w && b1 < n) p1 = *reinterpret_cast<const double2*>(S + roff(b1) + k0 + 2 * t);
+              if (b0 < n) p0 = *reinterpret_cast<const double2*>(S + roff(b0) + k0 + 2 * t);
+              if (b1 < n) p1 = *reinterpret_cast<const double2*>(S + roff(b1) + k0 + 2 * t);
               // W[2t][b] = -P[b][2t+1] x_t, W[2t+1][b] = P[b][2t] x_t
               w0[2 * t] = -p0.y * xv[t];
               w0[2 * t + 1] = p0.x * xv[t];
@@ -319,21 +379,36 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
               w1[2 * t + 1] = p1.x * xv[t];
             }
           }
-          const int ra = base + 64 * cb + 1 + rem;  // row a
-          const double* pa = S + roff(ra) + k0;
-          double* rowp = S + roff(ra);
-          const bool ok0 = b0 < ra, ok1 = b1 < ra;
-          double acc0 = ok0 ? rowp[b0] : 0.0, acc1 = ok1 ? rowp[b1] : 0.0;
+          const int ra = base + 64 * cb + 1 + 2 * rem;  // rows ra and ra + 1
+          const int rb = ra + 1 < n ? ra + 1 : ra;
+          double* rowa = S + roff(ra);
+          double* rowb = S + roff(rb);
+          const bool a0 = b0 < ra, a1 = b1 < ra, c0 = rb != ra && b0 < rb, c1 = rb != ra && b1 < rb;
+          double acc[4][2];
+          acc[0][0] = a0 ? rowa[b0] : 0.0;
+          acc[1][0] = a1 ? rowa[b1] : 0.0;
+          acc[2][0] = c0 ? rowb[b0] : 0.0;
+          acc[3][0] = c1 ? rowb[b1] : 0.0;
+#pragma unroll
+          for (int e = 0; e < 4; ++e) acc[e][1] = 0.0;
 #pragma unroll
           for (int i = 0; i < kPW; i += 2) {
-            const double2 v = *reinterpret_cast<const double2*>(pa + i);
-            acc0 = fma(v.x, w0[i], acc0);
-            acc1 = fma(v.x, w1[i], acc1);
-            acc0 = fma(v.y, w0[i + 1], acc0);
-            acc1 = fma(v.y, w1[i + 1], acc1);
+            const double2 pa = *reinterpret_cast<const double2*>(rowa + k0 + i);
+            const double2 pb = *reinterpret_cast<const double2*>(rowb + k0 + i);
+            const int h = (i >> 1) & 1;
+            acc[0][h] = fma(pa.x, w0[i], acc[0][h]);
+            acc[1][h] = fma(pa.x, w1[i], acc[1][h]);
+            acc[2][h] = fma(pb.x, w0[i], acc[2][h]);
+            acc[3][h] = fma(pb.x, w1[i], acc[3][h]);
+            acc[0][h] = fma(pa.y, w0[i + 1], acc[0][h]);
+            acc[1][h] = fma(pa.y, w1[i + 1], acc[1][h]);
+            acc[2][h] = fma(pb.y, w0[i + 1], acc[2][h]);
+            acc[3][h] = fma(pb.y, w1[i + 1], acc[3][h]);
           }
-          if (ok0) rowp[b0] = acc0;
-          if (ok1) rowp[b1] = acc1;
+          if (a0) rowa[b0] = acc[0][0] + acc[0][1];
+          if (a1) rowa[b1] = acc[1][0] + acc[1][1];
+          if (c0) rowb[b0] = acc[2][0] + acc[2][1];
+          if (c1) rowb[b1] = acc[3][0] + acc[3][1];
         }
       }
       __syncthreads();
