@@ -398,6 +398,65 @@ def measure_local_energy(args, dev, st) -> dict:
     return out
 
 
+def measure_config1(args, dev, st) -> dict:
+    """Config 1: 8x8 lattice (Pfaffians of 56 x 56), 1024 seeded configurations, no symmetry
+    projection: log|psi|, sign and local energy (U = 8, t' = -0.2).  GPU: one amplitude call and
+    one local-energy call per step, CUDA events, 3 steps after a warm-up.  CPU: the compiled
+    restatement (FP32 build, all host cores) on a bounded sample of the same configurations,
+    amplitudes of the samples and of every connected configuration; its local energies are
+    compared with the GPU's on that sample."""
+    import torch
+
+    import neuralhubbard_b200 as nh
+    from oracle import hubbard as ohub
+    from oracle import port
+
+    Lk, B = 8, 1024
+    Nk = Lk * Lk
+    nek = 7 * Nk // 16
+    params = nh.init_params(Lk, Lk, CHANNELS, LAYERS, std=0.02, seed=0)
+    state = nh.Variational(nh.PfaffianBackflow(Lk, Lk, nek, nek, params=params, device=dev),
+                           symm=False, max_parallel=B)
+    H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2])
+    s_np = nh.random_spins(np.random.default_rng(11), B, Nk, nek, nek)
+    s = torch.from_numpy(s_np).to(dev)
+    e = H.Oloc(state, nh.Samples(s, state(s)), count_connections=False)
+    torch.cuda.synchronize()
+    ev = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        psi = state(s)
+        e = H.Oloc(state, nh.Samples(s, psi), count_connections=False)
+        e1.record(st)
+        ev.append((e0, e1))
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / len(ev)
+    e_gpu = e.cpu().numpy()
+    out = {"lattice": "8x8", "configurations": B, "projected": False,
+           "gpu_ms_per_call": ms, "gpu_samples_per_s": B / (ms / 1e3),
+           "E_per_site": float(e_gpu.mean() / Nk)}
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except Exception:
+        cores = os.cpu_count() or 1
+    hp = dict(conv_w=[w.astype(np.float64) for w in params["conv_w"]],
+              conv_b=[b.astype(np.float64) for b in params["conv_b"]],
+              W=params["W"].astype(np.float64), theta=float(params["theta"]), Lx=Lk, Ly=Lk)
+    amp = lambda c: port.projected_amplitude(c, hp, symm=False, threads=cores, fp32=True)  # noqa
+    n_cpu = 16
+    t0 = time.perf_counter()
+    e_cpu = ohub.local_energy(s_np[:n_cpu], amp, Lk, Lk, 1.0, -0.2, 8.0)
+    wall = time.perf_counter() - t0
+    rate = n_cpu / wall
+    out["cpu"] = {"samples_per_s": rate, "cores": cores, "kind": "port (FP32 build)",
+                  "sample": f"{n_cpu} of the configurations ({wall:.1f} s)"}
+    out["gpu_over_cpu"] = out["gpu_samples_per_s"] / rate
+    out["eloc_max_rel_diff_vs_cpu_fp32"] = float(
+        np.max(np.abs(e_gpu[:n_cpu] - e_cpu) / np.maximum(1.0, np.abs(e_cpu))))
+    return out
+
+
 def _err_stats(la, l0, sg, s0) -> dict:
     e = np.abs(la - l0)
     return {"max": float(e.max()), "p99.9": float(np.quantile(e, 0.999)),
@@ -780,6 +839,9 @@ def run_ours(args) -> None:
     launches = sum(n for _, n in kern.values())
     kernels = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1]} for k, v in kern.items()}
 
+    config1 = None
+    if world == 1 and not args.no_config1:
+        config1 = measure_config1(args, dev, st)
     sampling = None
     q16 = None
     if world == 1 and not args.no_sampling:
@@ -827,6 +889,7 @@ def run_ours(args) -> None:
             "plain": plain,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": BATCH * 2 * N_SITES,
                     "d2h_bytes_per_step": BATCH * (4 + 8)},
+            "config1": config1,
             "sampling": sampling,
             "local_energy": local_energy,
             "large_lattice": large,
@@ -886,7 +949,6 @@ def run_reference(args) -> None:
 #   refine             16x16 projected amplitudes, 512 x 8 images, every image refined in FP64
 
 def _model(L, cnn_mode=0):
-
     import neuralhubbard_b200 as nh
 
     ne = 7 * L * L // 16
@@ -1044,6 +1106,8 @@ def main():
                     help="0: FP32 CUDA-core CNN (plain form); 1: tcgen05 BF16; 2: tcgen05 BF16x3")
     ap.add_argument("--pf-mode", type=int, default=0, choices=[0, 1],
                     help="0: CUDA-core Pfaffian; 1: matrix in tensor memory, tcgen05 updates")
+    ap.add_argument("--no-config1", action="store_true",
+                    help="skip the 8x8 amplitude + local-energy block (config 1)")
     ap.add_argument("--no-sampling", action="store_true",
                     help="skip the effective-samples comparison of the two sampler forms")
     ap.add_argument("--no-eloc", action="store_true",

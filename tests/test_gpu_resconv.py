@@ -160,3 +160,25 @@ def test_released_state_energy_tensor_cores():
     e = H.Oloc(state, nh.Samples(s, state(s))).cpu().numpy() / 256
     mean, err = e.mean(), e.std(ddof=1) / np.sqrt(len(e))
     assert abs(mean - info.energy) < 4 * err, (mean, err)
+
+
+def test_released_L24_state_energy():
+    """The released 24x24 state tpm02_L24_pfaffian (n = 504: the large-lattice Pfaffian and the
+    residual network with its activation planes in global memory) on 64 of its stored chains:
+    projected E/N within 4 standard errors of the published -0.74585(1) (code/states.py:118-119;
+    standard error from the published sigma^2/N = 0.0257)."""
+    name, L = "tpm02_L24_pfaffian", 24
+    eqx = os.path.join(RELEASED, name + ".eqx")
+    if not os.path.exists(eqx):
+        pytest.skip("released weights not fetched (tests/golden/fetch_released.py)")
+    info = checkpoint.RELEASED[name]
+    N = L * L
+    ne = 7 * N // 16
+    params = checkpoint.load_pfaffian_backflow(eqx, L, expect_md5=info.md5)
+    spins = checkpoint.load_spins(os.path.join(RELEASED, name + "_spins.npz"), N, ne, ne)
+    state = nh.Variational(nh.PfaffianBackflow(L, L, ne, ne, params=params))
+    H = nh.Hubbard(8.0, [1.0, info.tprime], [1, 2])
+    s = torch.from_numpy(spins[:64]).to(DEV)
+    e = H.Oloc(state, nh.Samples(s, state(s)), chunk_configs=2048).cpu().numpy() / N
+    err = np.sqrt(info.variance / N / len(e))
+    assert abs(e.mean() - info.energy) < 4 * err, (e.mean(), err)
