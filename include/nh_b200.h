@@ -164,6 +164,7 @@ enum {
   NH_K_RESCONV64 = 23,
   NH_K_RESCONV_TC = 24,
   NH_K_REFINE = 25,
+  NH_K_FUSED = 26,
   NH_K_COUNT = 32
 };
 int nh_profile_enable(int on);
@@ -241,12 +242,16 @@ int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_p
                  size_t workspace_bytes, void* stream);
 
 /* Local energies E_loc (batch,) FP64 of configurations with amplitudes (sign, logabs).  The
- * ragged list of connected configurations is evaluated in chunks of chunk_configs
- * configurations (0 = default) whose work counts stay on the device.  With n_conn_out null the
- * call never synchronises: its launch sequence depends only on the arguments (batch x
- * electrons x 8 / chunk chunks; the empty ones return at once), so a caller may record it into
- * a CUDA graph and replay it.  With n_conn_out set it synchronises the stream once, writes the
- * number of connections and launches only the chunks that hold connections. */
+ * ragged list of connected configurations (configuration x image x connection items) is
+ * evaluated, with chunk_configs <= 0, in one persistent pass: a fused kernel takes items off a
+ * device work counter and computes each item's features and FP32 Pfaffian in one block, the FP64
+ * refinement runs over device-built lists, and the launch sequence is the same whatever the
+ * number of connections (the backflow CNN with n <= 224; other networks fall back to chunks of
+ * 8192 configurations).  chunk_configs > 0 evaluates chunks of that many configurations with
+ * the unfused pipeline.  Work counts stay on the device either way.  With n_conn_out null the
+ * call never synchronises, so a caller may record it into a CUDA graph and replay it.  With
+ * n_conn_out set it synchronises the stream once, writes the number of connections and launches
+ * only the chunks that hold connections. */
 size_t nh_local_energy_workspace_bytes(int batch, int n_symm, int chunk_configs,
                                        const nh_backflow_params* p);
 int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs, int batch,

@@ -179,6 +179,7 @@ KERNEL_IDS = {
     "wtilde": 11, "pfaffian64": 12, "cnn64": 13, "flagged": 14, "pack": 15, "cnn_tc": 16,
     "pfaffian_tc": 17, "prop_sample": 18, "prop_forward": 19, "prop_backward": 20,
     "prop_adam": 21, "resconv": 22, "resconv64": 23, "resconv_tc": 24, "refine": 25,
+    "fused": 26,
 }
 K_COUNT = 32
 

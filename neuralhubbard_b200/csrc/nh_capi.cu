@@ -100,10 +100,10 @@ static size_t act_scratch_bytes(const nh_backflow_params& p) {
 }
 
 // Pivot-order records and refinement scratch: only where the FP64 refinement applies.
-static size_t refine_bytes(size_t items, int n) {
+static size_t refine_bytes(size_t items, int n, int d) {
   if (n > kRefineMaxN) return 0;
   return align256(items * perm_stride(n) * sizeof(uint16_t)) + align256(items * sizeof(int32_t)) +
-         align256(sizeof(int32_t)) + align256(refine_slice_bytes(n));
+         align256(sizeof(int32_t)) + align256(refine_slice_bytes(n, d));
 }
 
 size_t pipeline_bytes(int max_items, const nh_backflow_params& p) {
@@ -114,7 +114,7 @@ size_t pipeline_bytes(int max_items, const nh_backflow_params& p) {
          align256(it * sizeof(int32_t)) * 2 + align256(sizeof(int32_t)) +
          align256(it * n * d * sizeof(double)) + align256(it * n * sizeof(int32_t)) +
          align256(sizeof(int32_t)) + align256(pfaffian_scratch_bytes((int)n)) +
-         align256(act_scratch_bytes(p)) + align256(it * sizeof(float)) + refine_bytes(it, (int)n);
+         align256(act_scratch_bytes(p)) + align256(it * sizeof(float)) + refine_bytes(it, (int)n, (int)d);
 }
 
 PipelineBuffers carve_pipeline(void* ws, int max_items, const nh_backflow_params& prm) {
@@ -149,7 +149,7 @@ PipelineBuffers carve_pipeline(void* ws, int max_items, const nh_backflow_params
     b.perm = reinterpret_cast<uint16_t*>(take(it * perm_stride((int)n) * sizeof(uint16_t)));
     b.list32 = reinterpret_cast<int32_t*>(take(it * sizeof(int32_t)));
     b.count32 = reinterpret_cast<int32_t*>(take(sizeof(int32_t)));
-    b.slice = take(refine_slice_bytes((int)n));
+    b.slice = take(refine_slice_bytes((int)n, prm.channels / 2));
   }
   return b;
 }
@@ -225,6 +225,101 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
   }
   return launch_combine(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev, sign,
                         logabs, flags, p.cancel_tau, tc ? b.err : nullptr, st);
+}
+
+// ------------------------------------------------------------------ persistent (fused) pipeline
+// One fused launch computes every item's features and FP32 Pfaffian (items off a device work
+// counter), then the FP64 refinement runs over device lists with in-kernel features: no
+// per-item feature workspace, a launch sequence independent of the number of items.
+struct FusedBuffers {
+  float* pf_sign;
+  double* pf_logabs;
+  int32_t* pf_flags;
+  float* pf_ratio;
+  float* item_sign;
+  uint16_t* perm;
+  int32_t *list, *count, *list32, *count32, *queue;
+  void* slice;
+};
+
+static bool fused_ok(const nh_backflow_params& p) {
+  return fused_supported(p) && p.n_up + p.n_dn <= kRefineMaxN;
+}
+
+static size_t fused_bytes(size_t items, const nh_backflow_params& p) {
+  const int n = p.n_up + p.n_dn;
+  return align256(items * sizeof(float)) * 3 + align256(items * sizeof(double)) +
+         align256(items * sizeof(int32_t)) * 3 + align256(items * perm_stride(n) * 2) +
+         align256(sizeof(int32_t)) * 3 + align256(refine_slice_bytes(n, p.channels / 2));
+}
+
+static FusedBuffers carve_fused(void* ws, size_t items, const nh_backflow_params& p) {
+  const int n = p.n_up + p.n_dn;
+  char* q = static_cast<char*>(ws);
+  auto take = [&](size_t bytes) {
+    char* r = q;
+    q += align256(bytes);
+    return r;
+  };
+  FusedBuffers b;
+  b.pf_sign = reinterpret_cast<float*>(take(items * sizeof(float)));
+  b.pf_ratio = reinterpret_cast<float*>(take(items * sizeof(float)));
+  b.item_sign = reinterpret_cast<float*>(take(items * sizeof(float)));
+  b.pf_logabs = reinterpret_cast<double*>(take(items * sizeof(double)));
+  b.pf_flags = reinterpret_cast<int32_t*>(take(items * sizeof(int32_t)));
+  b.list = reinterpret_cast<int32_t*>(take(items * sizeof(int32_t)));
+  b.list32 = reinterpret_cast<int32_t*>(take(items * sizeof(int32_t)));
+  b.perm = reinterpret_cast<uint16_t*>(take(items * perm_stride(n) * 2));
+  b.count = reinterpret_cast<int32_t*>(take(sizeof(int32_t)));
+  b.count32 = reinterpret_cast<int32_t*>(take(sizeof(int32_t)));
+  b.queue = reinterpret_cast<int32_t*>(take(sizeof(int32_t)));
+  b.slice = take(refine_slice_bytes(n, p.channels / 2));
+  return b;
+}
+
+static int run_pipeline_fused(const ConfigList& cl, const nh_backflow_params& p,
+                              const FusedBuffers& b, float* sign, double* logabs, int32_t* flags,
+                              cudaStream_t st) {
+  const int n = p.n_up + p.n_dn, d = p.channels / 2;
+  const int max_items = cl.n_cfg * cl.G;
+  if (max_items <= 0) return NH_OK;
+  int rc;
+  FusedLaunch f{cl, &p, b.pf_sign, b.pf_logabs, b.pf_flags, b.pf_ratio, b.item_sign, b.perm,
+                b.queue};
+  if ((rc = launch_pfaffian_fused(f, st))) return rc;
+  const bool fp64 = p.Wt64 && (p.cond_tau > 0.0 || (p.cancel_tau > 0.0 && cl.G > 1));
+  if (fp64) {
+    if ((rc = launch_image_mark(b.pf_sign, b.pf_logabs, b.pf_flags, b.pf_ratio, cl.G, cl.n_cfg,
+                                cl.n_cfg_dev, p.cancel_tau, p.cond_tau, p.cond_tau > 1.0, st)))
+      return rc;
+    if ((rc = launch_flagged(b.pf_flags, max_items, cl.n_cfg_dev, cl.G, b.list, b.count, st)))
+      return rc;
+    RefineLaunch r{n, d, 4, nullptr, nullptr, nullptr, p.Wt64, p.Lx, p.Ly, b.list, b.count,
+                   max_items, b.perm, perm_stride(n), b.item_sign, b.pf_sign, b.pf_logabs,
+                   b.pf_flags, b.slice};
+    r.cl = cl;
+    r.cnn_w = p.conv_w_packed;
+    r.cnn_b = p.conv_b;
+    r.C = p.channels;
+    r.layers = p.layers;
+    if ((rc = launch_refine(r, st))) return rc;
+  }
+  if (p.refine_tau > 0.0) {
+    if ((rc = launch_flagged(b.pf_flags, max_items, cl.n_cfg_dev, cl.G, b.list32, b.count32, st,
+                             kFlagNeedRefine, NH_FLAG_ZERO_PIVOT | NH_FLAG_REFINED)))
+      return rc;
+    RefineLaunch r{n, d, 3, nullptr, nullptr, nullptr, p.Wt, p.Lx, p.Ly, b.list32, b.count32,
+                   max_items, b.perm, perm_stride(n), b.item_sign, b.pf_sign, b.pf_logabs,
+                   b.pf_flags, b.slice};
+    r.cl = cl;
+    r.cnn_w = p.conv_w_packed;
+    r.cnn_b = p.conv_b;
+    r.C = p.channels;
+    r.layers = p.layers;
+    if ((rc = launch_refine(r, st))) return rc;
+  }
+  return launch_combine(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev, sign,
+                        logabs, flags, p.cancel_tau, nullptr, st);
 }
 
 static int check_params(const nh_backflow_params* p) {
@@ -385,7 +480,7 @@ size_t nh_slogpf_workspace_bytes(int n, int batch) {
   const size_t b = (size_t)(batch > 0 ? batch : 1);
   const size_t ref = (ok && n <= kRefineMaxN)
                          ? align256(b * perm_stride(n) * sizeof(uint16_t)) +
-                               align256(refine_slice_bytes(n))
+                               align256(refine_slice_bytes(n, 16))
                          : 0;
   return tri + align256(b * sizeof(int32_t)) + align256(sizeof(int32_t)) + ref;
 }
@@ -490,18 +585,25 @@ static ElocLayout eloc_layout(void* ws, int batch, int n_symm, int chunk,
   L.to = reinterpret_cast<int32_t*>(take(cmax * 4));
   L.csign = reinterpret_cast<float*>(take(cmax * 4));
   L.clogabs = reinterpret_cast<double*>(take(cmax * 8));
-  L.n_chunks = (int)((cmax + chunk - 1) / chunk);
-  L.chunk_cnt = reinterpret_cast<int32_t*>(take((size_t)L.n_chunks * 4));
-  L.pipe = take(pipeline_bytes(chunk * n_symm, *p));
+  // chunk 0: the persistent path, one pass over the whole connection list
+  const size_t ch = chunk > 0 ? (size_t)chunk : cmax;
+  L.n_chunks = (int)((cmax + ch - 1) / ch);
+  L.chunk_cnt = reinterpret_cast<int32_t*>(take((size_t)(L.n_chunks > 0 ? L.n_chunks : 1) * 4));
+  L.pipe = take(chunk > 0 ? pipeline_bytes(chunk * n_symm, *p) : fused_bytes(cmax * n_symm, *p));
   L.bytes = off;
   return L;
+}
+
+// chunk_configs <= 0 selects the persistent path where the network supports it.
+static int eloc_chunk(int chunk_configs, const nh_backflow_params* p) {
+  if (chunk_configs > 0) return chunk_configs;
+  return fused_ok(*p) ? 0 : kDefaultChunk;
 }
 
 size_t nh_local_energy_workspace_bytes(int batch, int n_symm, int chunk_configs,
                                        const nh_backflow_params* p) {
   if (!p) return 0;
-  int chunk = chunk_configs > 0 ? chunk_configs : kDefaultChunk;
-  return eloc_layout(nullptr, batch, n_symm, chunk, p, 8).bytes;
+  return eloc_layout(nullptr, batch, n_symm, eloc_chunk(chunk_configs, p), p, 8).bytes;
 }
 
 int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs, int batch,
@@ -515,7 +617,7 @@ int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs
     return fail(NH_ERR_INVALID, "local_energy: bad buffers");
   if (n_symm != 1 && n_symm != 8) return fail(NH_ERR_INVALID, "local_energy: n_symm %d", n_symm);
   if (batch == 0) return NH_OK;
-  const int chunk = chunk_configs > 0 ? chunk_configs : kDefaultChunk;
+  const int chunk = eloc_chunk(chunk_configs, p);
   const size_t need = nh_local_energy_workspace_bytes(batch, n_symm, chunk, p);
   if ((rc = check_workspace(workspace, workspace_bytes, need, "local_energy"))) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -529,11 +631,13 @@ int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs
   if ((rc = launch_hop_emit(spins, batch, p->Lx, p->Ly, *h, L.offsets, cmax, nullptr, L.hval,
                             L.owner, L.from, L.to, st)))
     return rc;
-  // The ragged connection list is processed in chunks whose work counts live on the device, so
-  // the launch sequence does not depend on the data.  Without n_conn_out the call never waits
-  // for the GPU and runs all ceil(cmax / chunk) chunks (the empty ones exit at once); with it,
-  // the count is read back first and only the chunks that hold connections are launched.
-  if ((rc = launch_chunk_counts(L.offsets + batch, L.n_chunks, chunk, L.chunk_cnt, st)))
+  // The ragged connection list is processed in one persistent pass (chunk 0: items off a device
+  // work counter) or in chunks; either way the work counts live on the device, so the launch
+  // sequence does not depend on the data.  Without n_conn_out the call never waits for the GPU
+  // (chunked: all ceil(cmax / chunk) chunks run, the empty ones exit at once); with it, the count
+  // is read back first and only the chunks that hold connections are launched.
+  if ((rc = launch_chunk_counts(L.offsets + batch, L.n_chunks, chunk > 0 ? chunk : (int)cmax,
+                                L.chunk_cnt, st)))
     return rc;
   int used = L.n_chunks;
   if (n_conn_out) {
@@ -544,7 +648,16 @@ int nh_local_energy(const int8_t* spins, const float* sign, const double* logabs
       return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(st), "local_energy: sync"))) return rc;
     *n_conn_out = total;
-    used = (int)((total + chunk - 1) / chunk);
+    used = chunk > 0 ? (int)((total + chunk - 1) / chunk) : (total > 0 ? 1 : 0);
+  }
+  if (chunk == 0) {  // persistent: one fused pass over every connection
+    if (used > 0) {
+      ConfigList cl{spins, L.owner, L.from, L.to, L.chunk_cnt, (int)cmax, n_symm};
+      FusedBuffers fb = carve_fused(L.pipe, (size_t)cmax * n_symm, *p);
+      if ((rc = run_pipeline_fused(cl, *p, fb, L.csign, L.clogabs, nullptr, st))) return rc;
+    }
+    return launch_eloc_reduce(spins, sign, logabs, batch, N, h->U, L.offsets, L.hval, L.csign,
+                              L.clogabs, eloc, st);
   }
   PipelineBuffers b = carve_pipeline(L.pipe, chunk * n_symm, *p);
   for (int i = 0; i < used; ++i) {

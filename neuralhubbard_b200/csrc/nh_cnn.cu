@@ -13,6 +13,7 @@
 // descending-order convention).
 #include <math.h>
 
+#include "nh_cnn_item.cuh"
 #include "nh_common.cuh"
 
 namespace nh {
@@ -34,32 +35,6 @@ struct CnnArgs {
   float* item_sign;
   T* act;  // GACT: per-CTA activation planes (2 C (N + 1)) in global memory
 };
-
-__device__ __forceinline__ float gelu_tanh(float x) {
-  const float k0 = 0.7978845608028654f;  // sqrt(2 / pi)
-  return 0.5f * x * (1.0f + tanhf(k0 * (x + 0.044715f * x * x * x)));
-}
-__device__ __forceinline__ double gelu_tanh(double x) {
-  const double k0 = 0.7978845608028654;
-  return 0.5 * x * (1.0 + tanh(k0 * (x + 0.044715 * x * x * x)));
-}
-__device__ __forceinline__ float tfma(float a, float b, float c) { return fmaf(a, b, c); }
-__device__ __forceinline__ double tfma(double a, double b, double c) { return fma(a, b, c); }
-
-__device__ __forceinline__ void lds8(const float* p, float* o) {
-  const float4 a = reinterpret_cast<const float4*>(p)[0];
-  const float4 b = reinterpret_cast<const float4*>(p)[1];
-  o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
-  o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
-}
-__device__ __forceinline__ void lds8(const double* p, double* o) {
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const double2 v = reinterpret_cast<const double2*>(p)[k];
-    o[2 * k] = v.x;
-    o[2 * k + 1] = v.y;
-  }
-}
 
 // GACT: the two activation planes live in a per-CTA slice of global memory (large lattices,
 // where they exceed shared memory); shared memory then holds the weights and scratch only.
@@ -86,9 +61,6 @@ __global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
   const int G = a.cl.G;
   const int n_work = a.slot_item ? *a.slot_count
                                  : (a.cl.n_cfg_dev ? *a.cl.n_cfg_dev : a.cl.n_cfg) * G;
-  const int half = N / 2;
-  const int ngroups = C / 8;
-
   for (int slot = blockIdx.x; slot < n_work; slot += gridDim.x) {
     const int item = a.slot_item ? a.slot_item[slot] : slot;
     const int c = item / G, g = item - c * G;
@@ -98,71 +70,8 @@ __global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
     const int8_t* base = a.cl.spins + (int64_t)smp * M2;
 
     __syncthreads();  // previous item's readers of simg/act are done
-    for (int m = tid; m < M2; m += kNumThreads) {
-      const int src = sym_map(m, g, a.Lx, a.Ly, N);  // image[m] = s[g(m)] (g is an involution)
-      int v = base[src];
-      v = move_value(src, v, fr, to);
-      simg[m] = v > 0 ? 1 : -1;
-      const int ch = m >= N ? 1 : 0;
-      actA[ch * NS + (m - ch * N)] = v > 0 ? T(1) : T(-1);
-    }
-
-    T* in = actA;
-    T* out = actB;
-    int cin = 2;
-    const float* wl = a.wp;
-    for (int l = 0; l < a.layers; ++l) {
-      __syncthreads();
-      const int cnt = C * cin * 9;
-      for (int i = tid; i < cnt; i += kNumThreads) wsm[i] = T(__ldg(wl + i));
-      for (int i = tid; i < C; i += kNumThreads) bsm[i] = T(__ldg(a.b + l * C + i));
-      __syncthreads();
-      const bool act_fn = l < a.layers - 1;
-      for (int task = tid; task < ngroups * half; task += kNumThreads) {
-        const int grp = task / half;
-        const int s0 = task - grp * half, s1 = s0 + half;
-        const int x0 = s0 / a.Ly, y0 = s0 - x0 * a.Ly;
-        const int x1 = s1 / a.Ly, y1 = s1 - x1 * a.Ly;
-        T acc0[8], acc1[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc0[j] = acc1[j] = bsm[grp * 8 + j];
-        for (int ci = 0; ci < cin; ++ci) {
-          const T* inc = in + ci * NS;
-#pragma unroll
-          for (int u = 0; u < 3; ++u) {
-            int xa = x0 + u - 1, xb = x1 + u - 1;
-            xa = xa < 0 ? xa + a.Lx : (xa >= a.Lx ? xa - a.Lx : xa);
-            xb = xb < 0 ? xb + a.Lx : (xb >= a.Lx ? xb - a.Lx : xb);
-#pragma unroll
-            for (int v = 0; v < 3; ++v) {
-              int ya = y0 + v - 1, yb = y1 + v - 1;
-              ya = ya < 0 ? ya + a.Ly : (ya >= a.Ly ? ya - a.Ly : ya);
-              yb = yb < 0 ? yb + a.Ly : (yb >= a.Ly ? yb - a.Ly : yb);
-              const T i0 = inc[xa * a.Ly + ya];
-              const T i1 = inc[xb * a.Ly + yb];
-              T w8[8];
-              lds8(wsm + (ci * 9 + u * 3 + v) * C + grp * 8, w8);
-#pragma unroll
-              for (int j = 0; j < 8; ++j) {
-                acc0[j] = tfma(i0, w8[j], acc0[j]);
-                acc1[j] = tfma(i1, w8[j], acc1[j]);
-              }
-            }
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          out[(grp * 8 + j) * NS + s0] = act_fn ? gelu_tanh(acc0[j]) : acc0[j];
-          out[(grp * 8 + j) * NS + s1] = act_fn ? gelu_tanh(acc1[j]) : acc1[j];
-        }
-      }
-      wl += C * cin * 9;
-      cin = C;
-      T* t = in;
-      in = out;
-      out = t;
-    }
-    __syncthreads();
+    const T* in = cnn_layers<T>(a.wp, a.b, a.Lx, a.Ly, C, a.layers, base, fr, to, g, actA, actB,
+                                wsm, bsm, simg);
     const int d = C / 2;
     if (a.mode == 0) {
       float* dst = a.feat + (int64_t)item * C * N;

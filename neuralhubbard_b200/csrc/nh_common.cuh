@@ -262,7 +262,8 @@ __host__ __device__ __forceinline__ int perm_stride(int n) { return (n + 1 + 7) 
 struct RefineLaunch {
   int n, d;
   int mode;  // 0: dense FP32 F (items, n, n); 1: gather FP32 Y / idx (indexed by item);
-             // 2: gather FP64 Y64 / idx64 (indexed by slot) with Wt64
+             // 2: gather FP64 Y64 / idx64 (indexed by slot) with Wt64; 3 / 4: the item's FP32 /
+             // FP64 features computed in the kernel from cl (backflow CNN), gathered with Wt / Wt64
   const float* F;
   const void* Y;
   const int32_t* idx;
@@ -278,9 +279,13 @@ struct RefineLaunch {
   double* logabs;
   int32_t* flags;
   void* slice;  // refine_slice_bytes(n), required by the gather modes
+  ConfigList cl{};         // modes 3, 4
+  const float* cnn_w = nullptr;
+  const float* cnn_b = nullptr;
+  int C = 0, layers = 0;
 };
 int launch_refine(const RefineLaunch& q, cudaStream_t st);
-size_t refine_slice_bytes(int n);
+size_t refine_slice_bytes(int n, int d);
 
 size_t pipeline_bytes(int max_items, const nh_backflow_params& p);
 PipelineBuffers carve_pipeline(void* ws, int max_items, const nh_backflow_params& p);
@@ -333,6 +338,24 @@ int launch_pfaffian_from_F(const float* F, int n, int batch, const int32_t* list
                            float* sign, double* logabs, int32_t* flags, void* tri,
                            cudaStream_t st, uint16_t* perm = nullptr, double refine_tau = 0.0);
 int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st);
+// Features and FP32 Pfaffian of every item of a configuration list in one launch (the CNN of
+// each item runs in the block that factorises its pairing block; no feature workspace); items
+// come off the work counter queue (zeroed by the launch).  Writes per item: sign, logabs, flags,
+// pivot ratio, item sign and the pivot order.  fused_supported: the backflow CNN (not the
+// residual network), n <= 256.
+struct FusedLaunch {
+  ConfigList cl;
+  const nh_backflow_params* p;
+  float* sign;
+  double* logabs;
+  int32_t* flags;
+  float* ratio;
+  float* item_sign;
+  uint16_t* perm;
+  int32_t* queue;
+};
+bool fused_supported(const nh_backflow_params& p);
+int launch_pfaffian_fused(const FusedLaunch& f, cudaStream_t st);
 // Tensor-memory Pfaffian (one matrix per SM, trailing updates on tcgen05): mode 1 gathers from
 // g.Y / g.idx / g.Wt (FP32), mode 0 reads dense F (items, n, n) FP32.
 int launch_pfaffian_tc(const PfGatherArgs& g, int mode, const float* F, int32_t* err,

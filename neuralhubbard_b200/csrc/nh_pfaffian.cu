@@ -22,6 +22,7 @@
 
 #include <algorithm>
 
+#include "nh_cnn_item.cuh"
 #include "nh_common.cuh"
 
 namespace nh {
@@ -90,7 +91,58 @@ struct PfArgs {
   uint16_t* perm;            // or null: per item, logical -> physical row, then the parity
   double refine_tau;         // set kFlagNeedRefine when max|piv| > refine_tau min|piv| (0: off)
   float* ratio;              // or null: per item, max|piv| / min|piv| (inf for a zero pivot)
+  // mode 2 (features in the kernel): item = c * G + g of the configuration list; the CNN's
+  // occupied rows at byte y_off and their modes at idx_off of shared memory; rows >= tail_row
+  // of the triangle overlap the rows and are gathered through registers first.
+  ConfigList cl;
+  const float* cnn_w;   // packed weights [l][ci][tap][co]
+  const float* cnn_b;
+  int C, layers;
+  int y_off, idx_off, tail_row;
+  float* item_sign_out;  // (items,) the item signs the CNN phase computes
+  int32_t* queue;        // mode 2: work counter (zero before the launch)
 };
+
+// Shared-memory layout of the in-kernel CNN phase (mode 2): simg, occl (2N ints each), scan
+// scratch (4 Lx + 32 ints), activation planes A and B (C (N + 1) floats each), staged weights
+// (C * C * 9) and biases (C).  Returns the end of the activation planes; *end the whole extent.
+__host__ __device__ inline size_t cnn_phase_layout(int N, int C, int Lx, size_t* end) {
+  const size_t ints = 4 * (size_t)N + 4 * Lx + 32;
+  const size_t act0 = (sizeof(int) * ints + 15) & ~(size_t)15;
+  const size_t act_end = act0 + sizeof(float) * 2 * (size_t)C * (N + 1);
+  const size_t w0 = (act_end + 15) & ~(size_t)15;
+  *end = w0 + sizeof(float) * ((size_t)C * C * 9 + C);
+  return act_end;
+}
+
+// F[p][q] (p > q) of the item from occupied rows Y (n, D) and modes in shared memory, the same
+// arithmetic as pair_value: sum_a (Y[p, a] Y[q, a]) Wt[2 s_p + s_q, r(p, q), a] in order of a.
+template <int D>
+__device__ __forceinline__ float pair_smem(const float* yp, int mp, const float* __restrict__ Ys,
+                                           const int* __restrict__ ids, int q, int N, int Lx,
+                                           int Ly, const float* __restrict__ Wt) {
+  const int sp = mp >= N ? 1 : 0, sitep = mp - sp * N;
+  const int xp = sitep / Ly, ypos = sitep - xp * Ly;
+  const int mq = ids[q];
+  const int sq = mq >= N ? 1 : 0, siteq = mq - sq * N;
+  const int xq = siteq / Ly, yq = siteq - xq * Ly;
+  int dx = xp - xq, dy = ypos - yq;
+  dx += dx < 0 ? Lx : 0;
+  dy += dy < 0 ? Ly : 0;
+  const float* wrow = Wt + ((size_t)(2 * sp + sq) * N + dx * Ly + dy) * D;
+  const float* yq_row = Ys + q * D;
+  float acc = 0.0f;
+#pragma unroll
+  for (int a0 = 0; a0 < D; a0 += 4) {
+    const float4 w = __ldg(reinterpret_cast<const float4*>(wrow + a0));
+    const float4 v = *reinterpret_cast<const float4*>(yq_row + a0);
+    acc = fmaf(yp[a0] * v.x, w.x, acc);
+    acc = fmaf(yp[a0 + 1] * v.y, w.y, acc);
+    acc = fmaf(yp[a0 + 2] * v.z, w.z, acc);
+    acc = fmaf(yp[a0 + 3] * v.w, w.w, acc);
+  }
+  return acc;
+}
 
 __device__ __forceinline__ int tri_off(int i) { return (i * (i - 1)) >> 1; }
 
@@ -153,6 +205,90 @@ __device__ void gather_lower(T* Lw, int n, const T* __restrict__ Y, const int32_
   }
 }
 
+// Mode 2 load phase of one item: the CNN of its configuration in shared memory, its occupied rows
+// Y and modes written to shared memory (write_occupied_rows, item sign to item_sign_out), then
+// the gather of the lower triangle from them.  Rows of the triangle that overlap Y (tail_row on)
+// are computed into registers first and stored after a barrier.
+constexpr int kTailRegs = 16;
+
+template <int D>
+__device__ void features_and_gather(const PfArgs& a, int item, float* Lw, unsigned char* smem) {
+  const int n = a.n, N = a.Lx * a.Ly, C = a.C, M2 = 2 * N, NS = N + 1;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int G = a.cl.G;
+  const int c = item / G, g = item - c * G;
+  const int smp = a.cl.sample ? a.cl.sample[c] : c;
+  const int fr = a.cl.from ? a.cl.from[c] : -1;
+  const int to = a.cl.from ? a.cl.to[c] : -1;
+  const int8_t* base = a.cl.spins + (int64_t)smp * M2;
+  int* simg = reinterpret_cast<int*>(smem);
+  int* occl = simg + M2;
+  int* wbuf = occl + M2;
+  size_t cnn_end;
+  const size_t act_end = cnn_phase_layout(N, C, a.Lx, &cnn_end);
+  const size_t act0 = act_end - sizeof(float) * 2 * (size_t)C * NS;
+  float* actA = reinterpret_cast<float*>(smem + act0);
+  float* actB = actA + C * NS;
+  float* wsm = reinterpret_cast<float*>(smem + ((act_end + 15) & ~(size_t)15));
+  float* bsm = wsm + C * C * 9;
+  const float* in = cnn_layers<float>(a.cnn_w, a.cnn_b, a.Lx, a.Ly, C, a.layers, base, fr, to,
+                                      g, actA, actB, wsm, bsm, simg);
+  float* Ys = reinterpret_cast<float*>(smem + a.y_off);
+  int* ids = reinterpret_cast<int*>(smem + a.idx_off);
+  const int d = C / 2;
+  write_occupied_rows(simg, occl, wbuf, N, n, d, g, a.Lx, a.Ly, Ys, ids, a.item_sign_out + item,
+                      [&](int sg, int aa, int site) { return in[(sg * d + aa) * NS + site]; });
+  __syncthreads();
+  const float* Wt = static_cast<const float*>(a.Wt);
+  // rows below tail_row: straight into the triangle, warp <-> row, lane <-> column
+  for (int p = wid; p < a.tail_row; p += kNumThreads / 32) {
+    float yp[D];
+#pragma unroll
+    for (int a0 = 0; a0 < D; a0 += 4) {
+      const float4 v = *reinterpret_cast<const float4*>(Ys + p * D + a0);
+      yp[a0] = v.x;
+      yp[a0 + 1] = v.y;
+      yp[a0 + 2] = v.z;
+      yp[a0 + 3] = v.w;
+    }
+    const int mp = ids[p];
+    float* row = Lw + ((p * (p - 1)) >> 1);
+    for (int q = lane; q < p; q += 32) row[q] = pair_smem<D>(yp, mp, Ys, ids, q, N, a.Lx, a.Ly, Wt);
+  }
+  if (a.tail_row < n) {
+    // rows tail_row .. n-1 (E elements, at most kTailRegs per thread) through registers
+    const int t0 = (a.tail_row * (a.tail_row - 1)) >> 1;
+    const int E = ((n * (n - 1)) >> 1) - t0;
+    float v[kTailRegs];
+#pragma unroll
+    for (int k = 0; k < kTailRegs; ++k) {
+      const int e = tid + k * kNumThreads;
+      v[k] = 0.0f;
+      if (e < E) {
+        int p = a.tail_row;
+        while ((((p + 1) * p) >> 1) - t0 <= e) ++p;
+        const int q = e - ((((p * (p - 1)) >> 1)) - t0);
+        float yp[D];
+#pragma unroll
+        for (int a0 = 0; a0 < D; a0 += 4) {
+          const float4 y4 = *reinterpret_cast<const float4*>(Ys + p * D + a0);
+          yp[a0] = y4.x;
+          yp[a0 + 1] = y4.y;
+          yp[a0 + 2] = y4.z;
+          yp[a0 + 3] = y4.w;
+        }
+        v[k] = pair_smem<D>(yp, ids[p], Ys, ids, q, N, a.Lx, a.Ly, Wt);
+      }
+    }
+    __syncthreads();  // every read of Y is done
+#pragma unroll
+    for (int k = 0; k < kTailRegs; ++k) {
+      const int e = tid + k * kNumThreads;
+      if (e < E) Lw[t0 + e] = v[k];
+    }
+  }
+}
+
 // THREADS = 256: the lower triangle lives in shared memory (n <= 256).  THREADS = 1024 (large
 // lattices, n <= 1024): one thread per row as well, the triangle in a per-CTA slice of global
 // memory (a.tri; L2-resident up to n ~ 500), shared memory holding only the panel and the
@@ -186,14 +322,26 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
   int* rt = reinterpret_cast<int*>(rkey + WARPS);  // (warps) candidate row; later ballot counts
   int* rlog = rt + WARPS;                          // (warps) candidate logical label
   int* alist = rlog + WARPS;                       // (n) active physical rows
-  int* misc = alist + n;                            // [0] physical row of logical k
+  int* misc = alist + n;                            // [0] physical row of logical k, [1] item
 
   const int n_work = a.count_dev ? (*a.count_dev) * a.count_mult : a.n_slots;
   const T* Ybase = static_cast<const T*>(a.Y);
   const T* Wt = static_cast<const T*>(a.Wt);
-  for (int slot = blockIdx.x; slot < n_work; slot += gridDim.x) {
+  for (int slot = blockIdx.x;; slot += gridDim.x) {
+    if (a.queue) {  // dynamic schedule: the next item comes off the work counter
+      __syncthreads();
+      if (tid == 0) misc[1] = atomicAdd(a.queue, 1);
+      __syncthreads();
+      slot = misc[1];
+    }
+    if (slot >= n_work) break;
     const int item = a.slot_item ? a.slot_item[slot] : slot;
     __syncthreads();
+    if constexpr (sizeof(T) == 4 && THREADS == kNumThreads && D % 4 == 0) {
+      if (a.mode == 2) {
+        features_and_gather<D>(a, item, Lw, smem_raw);
+      }
+    }
     if (a.mode == 0) {
       const float* F = a.F + (size_t)item * n * n;
       for (int i = wid; i < n; i += WARPS) {
@@ -201,7 +349,7 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
         T* dst = Lw + tri_off(i);
         for (int j = lane; j < i; j += 32) dst[j] = T(__ldg(src + j));
       }
-    } else {
+    } else if (a.mode == 1) {
       gather_lower<T, D, WARPS>(Lw, n, Ybase + (size_t)slot * n * D, a.idx + (size_t)slot * n,
                                 Wt, a.Lx, a.Ly);
     }
@@ -411,7 +559,8 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
     if (tid == 0) {
       // Pfaffian = relabelling parity x product of the pivots, accumulated in FP64 as mantissa
       // and exponent; the pivot ratio flags near-nodal blocks.
-      float s = a.item_sign ? a.item_sign[item] : 1.0f;
+      const float* isg = a.mode == 2 ? a.item_sign_out : a.item_sign;
+      float s = isg ? isg[item] : 1.0f;
       double la, pmax_all = 0.0, pmin_all = 1.0;
       if (isnan(s)) flag |= NH_FLAG_NONFINITE;  // the CNN could not compute this item
       if (zero) {
@@ -461,7 +610,7 @@ size_t pf_smem(int n) {
   const size_t val_slots = sizeof(T) == 4 ? 0 : WARPS;
   return sizeof(T) * ((kGlobalTri ? 0 : ((tri + 3) & ~(size_t)3)) + 2 * (size_t)n * NB +
                       val_slots + ((n / 2 + 3) & ~(size_t)3)) +
-         sizeof(float) * WARPS + sizeof(int) * (2 * WARPS + (size_t)n + 1);
+         sizeof(float) * WARPS + sizeof(int) * (2 * WARPS + (size_t)n + 2);
 }
 
 // Large lattices: 1024 threads, triangle in a.tri; the panel width that fits shared memory.
@@ -1230,6 +1379,70 @@ int launch_pfaffian_gather(const PfGatherArgs& g, cudaStream_t st) {
   return g.fp64 ? launch_pf_d<double>(a, g.d, st) : launch_pf_d<float>(a, g.d, st);
 }
 
+// Fused features + FP32 Pfaffian (mode 2): shared-memory layout choice and launch.
+template <int NB, int D>
+int launch_fused_nb(PfArgs a, cudaStream_t st) {
+  const int n = a.n, N = a.Lx * a.Ly;
+  constexpr int WARPS = kWarps;
+  const size_t pf = pf_smem<float, NB>(n);
+  size_t cnn_end;
+  const size_t act_end = cnn_phase_layout(N, a.C, a.Lx, &cnn_end);
+  const size_t tri_pad = ((size_t)n * (n - 1) / 2 + 3) & ~(size_t)3;
+  const size_t tri_bytes = 4 * tri_pad, y_bytes = 4 * (size_t)n * D;
+  const size_t two_cta = 113 * 1024;
+  // A: rows after the triangle and the activation planes, modes after the rows.
+  const size_t yA = (std::max(act_end, tri_bytes) + 15) & ~(size_t)15;
+  const size_t totA = std::max(std::max(pf, cnn_end), yA + y_bytes + 4 * (size_t)n);
+  // B: rows in the triangle's tail (rows from tail_row gathered through registers), modes in the
+  // active-row list of the factorisation.
+  const size_t yB = (tri_bytes - y_bytes) & ~(size_t)15;
+  const size_t alist_off = 4 * (tri_pad + 2 * (size_t)n * NB + (((size_t)n / 2 + 3) & ~(size_t)3)) +
+                           4 * (size_t)WARPS * 3;
+  int tail = n;
+  if (y_bytes < tri_bytes) {
+    const size_t yf = yB / 4;
+    tail = 0;
+    while (tail < n && (size_t)tail * (tail - 1) / 2 + tail <= yf) ++tail;
+  }
+  const size_t tail_elems = (size_t)n * (n - 1) / 2 - (size_t)tail * (tail - 1) / 2;
+  const size_t totB = std::max(pf, cnn_end);
+  const bool okB = y_bytes < tri_bytes && yB >= act_end && alist_off >= act_end &&
+                   tail_elems <= (size_t)kTailRegs * kNumThreads;
+  size_t smem;
+  if (totA <= two_cta || !okB || totB > two_cta) {
+    smem = totA;
+    a.y_off = (int)yA;
+    a.idx_off = (int)(yA + y_bytes);
+    a.tail_row = n;
+  } else {
+    smem = totB;
+    a.y_off = (int)yB;
+    a.idx_off = (int)alist_off;
+    a.tail_row = tail;
+  }
+  if (smem > 227 * 1024)
+    return fail(NH_ERR_UNSUPPORTED, "fused amplitude: n=%d, N=%d needs %zu B of shared memory", n,
+                N, smem);
+  static size_t configured = 0;
+  if (smem > 48 * 1024 && smem > configured) {
+    cudaError_t e = cudaFuncSetAttribute(pfaffian_kernel<float, NB, D, kNumThreads>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return check_cuda(e, "fused amplitude smem attribute");
+    configured = smem;
+  }
+  const int per_sm = smem <= two_cta ? 2 : 1;
+  int grid = num_sms() * per_sm;
+  if (grid > a.n_slots) grid = a.n_slots;
+  if (grid <= 0) return NH_OK;
+  if (a.queue) {
+    cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(int32_t), st);
+    if (e != cudaSuccess) return check_cuda(e, "fused amplitude: clear work counter");
+  }
+  ProfScope prof_scope(NH_K_FUSED, st);
+  pfaffian_kernel<float, NB, D, kNumThreads><<<grid, kNumThreads, smem, st>>>(a);
+  return check_launch("pfaffian_kernel (fused features)");
+}
+
 int launch_pfaffian_tc(const PfGatherArgs& g, int mode, const float* F, int32_t* err,
                        cudaStream_t st) {
   if (g.n <= 0 || g.n % 2 || g.n > kNumThreads)
@@ -1280,6 +1493,47 @@ int launch_pairing_smem(const float* Y, const int32_t* idx, const float* Wt, int
   ProfScope prof_scope(NH_K_PAIRING, st);
   pairing_smem_kernel<D><<<grid, kNumThreads, smem, st>>>(Y, idx, Wt, Lx, Ly, n, batch, F);
   return check_launch("pairing_smem_kernel");
+}
+
+bool fused_supported(const nh_backflow_params& p) {
+  const int n = p.n_up + p.n_dn, N = p.Lx * p.Ly, d = p.channels / 2;
+  return p.net == NH_NET_CNN && n <= kNumThreads && n % 2 == 0 && N % 2 == 0 &&
+         p.channels % 16 == 0 && p.channels <= 64 && (d == 8 || d == 16 || d == 32);
+}
+
+int launch_pfaffian_fused(const FusedLaunch& f, cudaStream_t st) {
+  const nh_backflow_params& p = *f.p;
+  if (!fused_supported(p)) return fail(NH_ERR_UNSUPPORTED, "fused amplitude: unsupported network");
+  PfArgs a{};
+  a.n = p.n_up + p.n_dn;
+  a.mode = 2;
+  a.Wt = p.Wt;
+  a.Lx = p.Lx;
+  a.Ly = p.Ly;
+  a.count_dev = f.cl.n_cfg_dev;
+  a.count_mult = f.cl.G;
+  a.n_slots = f.cl.n_cfg * f.cl.G;
+  a.sign = f.sign;
+  a.logabs = f.logabs;
+  a.flags = f.flags;
+  a.cond_tau = p.cond_tau;
+  a.perm = f.perm;
+  a.refine_tau = p.refine_tau;
+  a.ratio = f.ratio;
+  a.cl = f.cl;
+  a.cnn_w = p.conv_w_packed;
+  a.cnn_b = p.conv_b;
+  a.C = p.channels;
+  a.layers = p.layers;
+  a.item_sign_out = f.item_sign;
+  a.queue = f.queue;
+  const bool nb8 = pf_smem<float, 8>(a.n) <= 113 * 1024;
+  switch (p.channels / 2) {
+    case 8: return nb8 ? launch_fused_nb<8, 8>(a, st) : launch_fused_nb<4, 8>(a, st);
+    case 16: return nb8 ? launch_fused_nb<8, 16>(a, st) : launch_fused_nb<4, 16>(a, st);
+    case 32: return nb8 ? launch_fused_nb<8, 32>(a, st) : launch_fused_nb<4, 32>(a, st);
+    default: return fail(NH_ERR_UNSUPPORTED, "fused amplitude: d=%d", p.channels / 2);
+  }
 }
 
 int launch_pairing(const float* Y, const int32_t* idx, const float* Wt, int Lx, int Ly, int d,

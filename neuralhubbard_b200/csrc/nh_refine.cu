@@ -25,6 +25,7 @@
 
 #include <algorithm>
 
+#include "nh_cnn_item.cuh"
 #include "nh_common.cuh"
 
 namespace nh {
@@ -36,11 +37,25 @@ constexpr int kPW = 8;  // panel width: 4 elimination steps
 
 // Row a of the padded lower triangle starts at roff(a) (even, so FP64 pairs are 16-byte aligned).
 __host__ __device__ __forceinline__ int roff(int a) { return (a * (a - 1)) / 2 + a / 2; }
+// Elements of a whole triangle, rounded up to a multiple of 4 so that every per-CTA slice (FP32
+// or FP64) and every 16-byte vector of the copies stays aligned.
+__host__ __device__ __forceinline__ int tri_elems(int n) { return (roff(n) + 3) & ~3; }
+// Bytes of one CTA's slice: the FP64 triangle, or an item's FP64 rows and modes (modes 3, 4),
+// whichever is larger; a multiple of 16.
+__host__ __device__ __forceinline__ size_t slice_stride(int n, int d) {
+  const size_t tri = 8 * (size_t)tri_elems(n), rows = 8 * (size_t)n * d + 4 * (size_t)n;
+  return ((tri > rows ? tri : rows) + 15) & ~(size_t)15;
+}
 
 struct RefineArgs {
   int n;
   int mode;  // 0: dense FP32 F (items, n, n); 1: gather FP32 (Y, idx by item); 2: gather FP64
-             // (Y64, idx64 by slot, Wt64)
+             // (Y64, idx64 by slot, Wt64); 3 / 4: FP32 / FP64 features computed in the kernel
+             // from the configuration list, then gathered (Wt / Wt64)
+  ConfigList cl;       // modes 3, 4
+  const float* cnn_w;  // modes 3, 4: packed weights [l][ci][tap][co]
+  const float* cnn_b;
+  int C, layers;
   const float* F;
   const void* Y;
   const int32_t* idx;
@@ -55,7 +70,7 @@ struct RefineArgs {
   float* sign;
   double* logabs;
   int32_t* flags;
-  double* slice;  // per CTA: roff(n) doubles
+  void* slice;  // per CTA: slice_stride(n, D) bytes
 };
 
 template <typename T>
@@ -75,23 +90,21 @@ struct Vec2<double> {
 // (element type T).  Warp <-> 32 consecutive logical columns q (their features in registers
 // when small), rows p > q in turn (the row's features broadcast); each element reads one Wt row.
 template <typename T, int D>
-__device__ void gather_permuted(const RefineArgs& a, int item, int slot, const int* perm,
-                                unsigned char* smem, T* slice) {
+__device__ void gather_permuted(const RefineArgs& a, const T* Yg, const int32_t* ig,
+                                const int* perm, unsigned char* smem, T* slice) {
   const int n = a.n, N = a.Lx * a.Ly;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   constexpr int DP = D + (sizeof(T) == 4 ? 4 : 2);
   constexpr int VK = Vec2<T>::k;
   using V = typename Vec2<T>::V;
-  const int base = a.mode == 2 ? slot : item;
-  const T* Yg = static_cast<const T*>(a.Y) + (size_t)base * n * D;
-  const int32_t* ig = a.idx + (size_t)base * n;
   const T* Wg = static_cast<const T*>(a.Wt);
   T* ys = reinterpret_cast<T*>(smem);                    // (n, DP)
   int* info = reinterpret_cast<int*>(ys + n * DP);       // (n) spin << 16 | x << 8 | y
   T* wts = reinterpret_cast<T*>(info + ((n + 3) & ~3));  // (4 N, DP) when staged
   // Row r of the source (D values, 16-byte vectors) to row r of the padded staging copy; several
-  // vectors in flight per thread.
-  auto stage = [&](const T* src, T* dst, int rows) {
+  // vectors in flight per thread.  Read-only tables (nc) take the non-coherent path; the rows,
+  // which modes 3 and 4 write in this kernel, plain loads.
+  auto stage = [&](const T* src, T* dst, int rows, bool nc) {
     constexpr int VPR = D / VK;  // vectors per row
     const int nv = rows * VPR;
     for (int v0 = tid; v0 < nv; v0 += 4 * kRThreads) {
@@ -99,7 +112,8 @@ __device__ void gather_permuted(const RefineArgs& a, int item, int slot, const i
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const int v = v0 + u * kRThreads;
-        if (v < nv) buf[u] = __ldg(reinterpret_cast<const V*>(src) + v);
+        if (v < nv) buf[u] = nc ? __ldg(reinterpret_cast<const V*>(src) + v)
+                                : reinterpret_cast<const V*>(src)[v];
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
@@ -111,13 +125,13 @@ __device__ void gather_permuted(const RefineArgs& a, int item, int slot, const i
       }
     }
   };
-  stage(Yg, ys, n);
+  stage(Yg, ys, n, false);
   for (int p = tid; p < n; p += kRThreads) {
     const int m = ig[p];
     const int sp = m >= N ? 1 : 0, site = m - sp * N, x = site / a.Ly;
     info[p] = (sp << 16) | (x << 8) | (site - x * a.Ly);
   }
-  if (a.stage_wt) stage(Wg, wts, 4 * N);
+  if (a.stage_wt) stage(Wg, wts, 4 * N, true);
   __syncthreads();
   int total = 0;
   for (int qb = 0; 32 * qb + 1 < n; ++qb) total += n - 32 * qb - 1;
@@ -178,8 +192,8 @@ __device__ void gather_permuted(const RefineArgs& a, int item, int slot, const i
   }
 }
 
-// The CTA's slice (tot values, tot a multiple of 4) into the FP64 triangle, 16-byte vectors with
-// four in flight per thread.
+// The CTA's slice (tot = tri_elems(n) values, a multiple of 4) into the FP64 triangle, 16-byte
+// vectors with four in flight per thread.
 __device__ __forceinline__ void copy_slice(const float* sl, double* S, int tot) {
   const int nv = tot / 4;
   for (int v0 = threadIdx.x; v0 < nv; v0 += 4 * kRThreads) {
@@ -208,6 +222,45 @@ __device__ __forceinline__ void copy_slice(const double* sl, double* S, int tot)
     for (int u = 0; u < 4; ++u)
       if (v0 + u * kRThreads < nv) reinterpret_cast<double2*>(S)[v0 + u * kRThreads] = buf[u];
   }
+}
+
+// Modes 3 and 4: the features of the item's configuration (CNN in shared memory) written as its
+// occupied rows Y (n, d) and modes to global memory (the CTA's slice, read back by the gather's
+// staging before the gather overwrites it).
+template <typename T>
+__device__ void features_to(const RefineArgs& a, int item, unsigned char* smem, T* Ydst,
+                            int32_t* idst) {
+  const int N = a.Lx * a.Ly, C = a.C, M2 = 2 * N, NS = N + 1;
+  const int G = a.cl.G;
+  const int c = item / G, g = item - c * G;
+  const int smp = a.cl.sample ? a.cl.sample[c] : c;
+  const int fr = a.cl.from ? a.cl.from[c] : -1;
+  const int to = a.cl.from ? a.cl.to[c] : -1;
+  const int8_t* base = a.cl.spins + (int64_t)smp * M2;
+  __shared__ float sign_dummy;
+  int* simg = reinterpret_cast<int*>(smem);
+  int* occl = simg + M2;
+  int* wbuf = occl + M2;
+  const size_t ints = 4 * (size_t)N + 4 * a.Lx + 32;
+  T* actA = reinterpret_cast<T*>(smem + ((sizeof(int) * ints + 15) & ~(size_t)15));
+  T* actB = actA + C * NS;
+  T* wsm = actB + C * NS;
+  wsm = reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(wsm) + 15) & ~(uintptr_t)15);
+  T* bsm = wsm + C * C * 9;
+  __syncthreads();
+  const T* in = cnn_layers<T>(a.cnn_w, a.cnn_b, a.Lx, a.Ly, C, a.layers, base, fr, to, g, actA,
+                              actB, wsm, bsm, simg);
+  const int d = C / 2;
+  write_occupied_rows(simg, occl, wbuf, N, a.n, d, g, a.Lx, a.Ly, Ydst, idst, &sign_dummy,
+                      [&](int sg, int aa, int site) { return in[(sg * d + aa) * NS + site]; });
+  __syncthreads();
+}
+
+// Shared memory of the in-kernel CNN (modes 3, 4).
+size_t features_smem(int N, int C, int Lx, int elt) {
+  const size_t ints = 4 * (size_t)N + 4 * Lx + 32;
+  const size_t act = ((sizeof(int) * ints + 15) & ~(size_t)15) + (size_t)elt * 2 * C * (N + 1);
+  return ((act + 15) & ~(size_t)15) + (size_t)elt * ((size_t)C * C * 9 + C);
 }
 
 template <int D>
@@ -240,15 +293,30 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
         }
       }
     } else {
-      const int tot = roff(n);
-      if (a.mode == 1) {
-        float* sl = reinterpret_cast<float*>(a.slice) + (size_t)blockIdx.x * tot;
-        gather_permuted<float, D>(a, item, slot, perm_s, smem, sl);
+      const int tot = tri_elems(n);  // a multiple of 4
+      unsigned char* slb = static_cast<unsigned char*>(a.slice) + (size_t)blockIdx.x * slice_stride(n, D);
+      if (a.mode == 1 || a.mode == 3) {
+        float* sl = reinterpret_cast<float*>(slb);
+        const float* Yg = static_cast<const float*>(a.Y) + (size_t)item * n * D;
+        const int32_t* ig = a.idx + (size_t)item * n;
+        if (a.mode == 3) {  // the item's FP32 features, rows and modes to the slice
+          features_to(a, item, smem, sl, reinterpret_cast<int32_t*>(sl + n * D));
+          Yg = sl;
+          ig = reinterpret_cast<const int32_t*>(sl + n * D);
+        }
+        gather_permuted<float, D>(a, Yg, ig, perm_s, smem, sl);
         __syncthreads();  // slice written; the staging area is dead
         copy_slice(sl, S, tot);
       } else {
-        double* sl = a.slice + (size_t)blockIdx.x * tot;
-        gather_permuted<double, D>(a, item, slot, perm_s, smem, sl);
+        double* sl = reinterpret_cast<double*>(slb);
+        const double* Yg = static_cast<const double*>(a.Y) + (size_t)slot * n * D;
+        const int32_t* ig = a.idx + (size_t)slot * n;
+        if (a.mode == 4) {
+          features_to(a, item, smem, sl, reinterpret_cast<int32_t*>(sl + n * D));
+          Yg = sl;
+          ig = reinterpret_cast<const int32_t*>(sl + n * D);
+        }
+        gather_permuted<double, D>(a, Yg, ig, perm_s, smem, sl);
         __syncthreads();
         copy_slice(sl, S, tot);
       }
@@ -442,12 +510,13 @@ size_t stage_bytes(int n, int N, int D, int elt, bool wt) {
 template <int D>
 int launch_refine_d(RefineArgs a, int max_slots, cudaStream_t st) {
   const int N = a.Lx * a.Ly;
-  const size_t tri = sizeof(double) * roff(a.n);
+  const size_t tri = sizeof(double) * tri_elems(a.n);
   size_t smem = tri;
   if (a.mode != 0) {
-    const int elt = a.mode == 1 ? 4 : 8;
+    const int elt = (a.mode == 1 || a.mode == 3) ? 4 : 8;
     a.stage_wt = stage_bytes(a.n, N, D, elt, true) <= kRefineSmemLimit;
     smem = std::max(smem, stage_bytes(a.n, N, D, elt, a.stage_wt));
+    if (a.mode >= 3) smem = std::max(smem, features_smem(N, a.C, a.Lx, elt));
   }
   if (smem > kRefineSmemLimit)
     return fail(NH_ERR_UNSUPPORTED, "refine: n=%d needs %zu B of shared memory", a.n, smem);
@@ -468,8 +537,8 @@ int launch_refine_d(RefineArgs a, int max_slots, cudaStream_t st) {
 
 }  // namespace
 
-size_t refine_slice_bytes(int n) {
-  return (n > 0 && n <= kRefineMaxN) ? (size_t)num_sms() * roff(n) * sizeof(double) : 0;
+size_t refine_slice_bytes(int n, int d) {
+  return (n > 0 && n <= kRefineMaxN) ? (size_t)num_sms() * slice_stride(n, d < 8 ? 8 : d) : 0;
 }
 
 int launch_refine(const RefineLaunch& q, cudaStream_t st) {
@@ -495,7 +564,14 @@ int launch_refine(const RefineLaunch& q, cudaStream_t st) {
   a.sign = q.sign;
   a.logabs = q.logabs;
   a.flags = q.flags;
-  a.slice = static_cast<double*>(q.slice);
+  a.slice = q.slice;
+  a.cl = q.cl;
+  a.cnn_w = q.cnn_w;
+  a.cnn_b = q.cnn_b;
+  a.C = q.C;
+  a.layers = q.layers;
+  if (q.mode >= 3 && (!q.cnn_w || !q.cnn_b || q.C % 16 || q.d * 2 != q.C))
+    return fail(NH_ERR_INVALID, "refine: in-kernel features need the CNN weights");
   switch (q.mode == 0 ? 16 : q.d) {
     case 8: return launch_refine_d<8>(a, q.max_slots, st);
     case 16: return launch_refine_d<16>(a, q.max_slots, st);
