@@ -475,15 +475,15 @@ def measure_precision(dev, st, spins, flush) -> dict:
 
     params = nh.init_params(L, L, CHANNELS, LAYERS, std=0.02, seed=0)
     forms = [("all FP64 (cond_tau 1, reference)", dict(cnn_mode=0, cond_tau=1.0)),
-             ("FP32 CNN, FP64 recompute of pivot ratio > 100 only",
-              dict(cnn_mode=0, cancel_tau=0.0)),
-             ("tcgen05 BF16x3 CNN, FP64 recompute of pivot ratio > 100 only",
-              dict(cnn_mode=2, cancel_tau=0.0)),
-             ("plain (defaults): FP32 CNN, FP64 recompute of pivot ratio > 100 and of "
-              "configurations cancelling > 8x", dict(cnn_mode=0)),
-             ("chosen (defaults): tcgen05 BF16x3 CNN, same recompute", dict(cnn_mode=2)),
-             ("tcgen05 BF16x3 CNN, no FP64 recompute", dict(cnn_mode=2, cond_tau=0.0,
-                                                             cancel_tau=0.0)),
+             ("plain (defaults): FP32 CNN; FP64 features + static-pivot FP64 refinement of "
+              "images with |share| x pivot ratio > 5 and of cancelling configurations",
+              dict(cnn_mode=0)),
+             ("chosen (defaults): tcgen05 BF16x3 CNN, same policy", dict(cnn_mode=2)),
+             ("tcgen05 BF16x3 CNN, threshold 10", dict(cnn_mode=2, cond_tau=10.0)),
+             ("tcgen05 BF16x3 CNN, threshold 5 + FP32-block refinement of every image",
+              dict(cnn_mode=2, refine_tau=1.0)),
+             ("tcgen05 BF16x3 CNN, no FP64 work", dict(cnn_mode=2, cond_tau=0.0,
+                                                       cancel_tau=0.0)),
              ("tcgen05 CNN + tensor-memory 3xTF32 Pfaffian (pf_mode 1)",
               dict(cnn_mode=2, pf_mode=1))]
     out = {}

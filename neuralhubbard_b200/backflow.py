@@ -117,14 +117,19 @@ def pairing_occ(Y: torch.Tensor, idx: torch.Tensor, Wt: torch.Tensor, geom: Pair
     return F
 
 
-DEFAULT_COND_TAU = 100.0
+# FP64 features (and an FP64 refinement of the log-Pfaffian against the FP64 pairing block) for
+# every image whose estimated error |w_g| x pivot ratio exceeds this; w_g is the image's signed
+# share of the projected amplitude (1 without projection).  5 keeps log|psi| within 1e-4 of FP64
+# on every configuration of the 16x16 benchmark set for both CNN forms.
+DEFAULT_COND_TAU = 5.0
 # Projected amplitudes whose 8 images cancel by more than this factor are recomputed in FP64:
 # the cancellation amplifies the FP32 error of the images by the same factor.
 DEFAULT_CANCEL_TAU = 8.0
 # Images whose FP32 pivot ratio exceeds this are refined in FP64 with their FP32 pivot order
-# (a blocked static-pivot elimination, no pivot search): it removes the FP32 factorisation
-# error, the dominant error of an FP32 log-Pfaffian at n = 224.
-DEFAULT_REFINE_TAU = 10.0
+# against their own FP32 pairing block (a blocked static-pivot elimination, no pivot search):
+# it removes the FP32 factorisation error.  Off by default: the images whose error matters
+# already get FP64 features and the same refinement through cond_tau.
+DEFAULT_REFINE_TAU = 0.0
 
 
 def slogpf(F: torch.Tensor, cond_tau: float = DEFAULT_COND_TAU):

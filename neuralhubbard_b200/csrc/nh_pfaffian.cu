@@ -21,6 +21,8 @@
 #include <math.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "nh_cnn_item.cuh"
 #include "nh_common.cuh"
@@ -613,6 +615,24 @@ size_t pf_smem(int n) {
          sizeof(float) * WARPS + sizeof(int) * (2 * WARPS + (size_t)n + 2);
 }
 
+// Raises a kernel's dynamic shared-memory cap to the largest the launches need, never lowering
+// it: the plain and the fused launchers share kernel instantiations, and a cap set lower by one
+// would make the other's launch fail.  One cap per kernel, under a lock.
+template <typename K>
+int raise_smem_cap(K* kernel, size_t smem) {
+  static std::mutex mu;
+  static std::map<const void*, size_t> caps;
+  if (smem <= 48 * 1024) return NH_OK;
+  std::lock_guard<std::mutex> g(mu);
+  size_t& cap = caps[reinterpret_cast<const void*>(kernel)];
+  if (smem <= cap) return NH_OK;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return check_cuda(e, "pfaffian kernel shared-memory attribute");
+  cap = smem;
+  return NH_OK;
+}
+
 // Large lattices: 1024 threads, triangle in a.tri; the panel width that fits shared memory.
 constexpr int kBigThreads = 1024;
 constexpr int kBigNB = 4;
@@ -625,13 +645,7 @@ int launch_pf(const PfArgs& a, cudaStream_t st) {
     return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d needs %zu B of shared memory", a.n, smem);
   if (kGlobalTri && !a.tri)
     return fail(NH_ERR_UNSUPPORTED, "slogpf: n=%d needs the large-lattice scratch", a.n);
-  static size_t configured = 0;
-  if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pfaffian_kernel<T, NB, D, THREADS>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "slogpf smem attribute");
-    configured = smem;
-  }
+  if (int rc = raise_smem_cap(pfaffian_kernel<T, NB, D, THREADS>, smem)) return rc;
   const int per_sm = (!kGlobalTri && smem <= 113 * 1024) ? 2 : 1;
   int grid = num_sms() * per_sm;
   if (grid > a.n_slots) grid = a.n_slots;
@@ -1423,13 +1437,7 @@ int launch_fused_nb(PfArgs a, cudaStream_t st) {
   if (smem > 227 * 1024)
     return fail(NH_ERR_UNSUPPORTED, "fused amplitude: n=%d, N=%d needs %zu B of shared memory", n,
                 N, smem);
-  static size_t configured = 0;
-  if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pfaffian_kernel<float, NB, D, kNumThreads>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return check_cuda(e, "fused amplitude smem attribute");
-    configured = smem;
-  }
+  if (int rc = raise_smem_cap(pfaffian_kernel<float, NB, D, kNumThreads>, smem)) return rc;
   const int per_sm = smem <= two_cta ? 2 : 1;
   int grid = num_sms() * per_sm;
   if (grid > a.n_slots) grid = a.n_slots;

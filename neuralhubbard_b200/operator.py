@@ -46,19 +46,23 @@ class Hubbard:
     def c_params(self) -> _lib.HubbardParams:
         return _lib.HubbardParams(self.t, self.tp, self.U, self.n_dirs)
 
-    def Oloc(self, state: Variational, samples: Samples, chunk_configs: int = 0,
+    def Oloc(self, state: Variational, samples: Samples, chunk_configs: Optional[int] = None,
              count_connections: bool = True) -> torch.Tensor:
         """(B,) FP64 local energies E_loc(s) = sum_s' <s|H|s'> psi(s') / psi(s).
 
-        ``chunk_configs`` = 0 takes the size ``autotune`` picked for this lattice and form (the
-        library default if none).  With ``count_connections`` the call waits once for the number
-        of connections (kept in ``last_n_conn``) and launches only the chunks that hold some;
-        without it, it never waits for the GPU and can be captured in a CUDA graph."""
+        ``chunk_configs``: 0 evaluates every connected configuration in one persistent pass (a
+        fused kernel taking (configuration, image, connection) items off a device work counter;
+        the backflow CNN with n <= 224, else the library's chunks); > 0 evaluates chunks of that
+        many configurations; None takes what ``autotune`` picked for this lattice and form (the
+        persistent pass if nothing was tuned).  With ``count_connections`` the call waits once
+        for the number of connections (kept in ``last_n_conn``); without it, it never waits for
+        the GPU and can be captured in a CUDA graph."""
         spins = as_spins(samples.spins, state.device)
         psi = samples.psi if samples.psi is not None else state(spins)
         B = spins.shape[0]
-        if chunk_configs <= 0:
+        if chunk_configs is None:
             chunk_configs = _CHUNK_CACHE.get(_tune_key(state, self), 0)
+        chunk_configs = max(0, int(chunk_configs))
         eloc = torch.empty(B, dtype=torch.float64, device=state.device)
         p = state.model.c_params()
         h = self.c_params()
@@ -75,10 +79,11 @@ class Hubbard:
         return eloc
 
     def autotune(self, state: Variational, samples: Samples,
-                 candidates: Sequence[int] = (2048, 8192, 32768), repeats: int = 2) -> int:
-        """Time ``Oloc`` on ``samples`` for each chunk size (CUDA events, after one warm-up
-        call each), remember the fastest for this lattice, symmetry and precision form, and
-        return it.  Later ``Oloc`` calls with ``chunk_configs`` = 0 use it."""
+                 candidates: Sequence[int] = (0, 2048, 8192, 32768), repeats: int = 2) -> int:
+        """Time ``Oloc`` on ``samples`` for each evaluation shape (0: the persistent fused pass;
+        else chunks of that many configurations), CUDA events after one warm-up call each;
+        remember the fastest for this lattice, neighbour range, symmetry and precision form,
+        and return it.  Later ``Oloc`` calls without ``chunk_configs`` use it."""
         best, best_ms = 0, float("inf")
         st = torch.cuda.current_stream(state.device)
         for c in candidates:
