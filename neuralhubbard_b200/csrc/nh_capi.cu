@@ -186,9 +186,13 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
     g.perm = b.perm;
     g.refine_tau = p.refine_tau;
   }
-  if ((rc = p.pf_mode == 1 ? launch_pfaffian_tc(g, 1, nullptr, b.err, st)
-                           : launch_pfaffian_gather(g, st)))
-    return rc;
+  if (p.pf_mode == 1)
+    rc = launch_pfaffian_tc(g, 1, nullptr, b.err, st);
+  else if (staged_supported(g))
+    rc = launch_pfaffian_staged(g, st);
+  else
+    rc = launch_pfaffian_gather(g, st);
+  if (rc) return rc;
   const bool fp64 = p.Wt64 && (p.cond_tau > 0.0 || (p.cancel_tau > 0.0 && cl.G > 1));
   if (fp64) {
     // cond_tau <= 1 flags every image (the all-FP64 form): no weighting then.
@@ -320,6 +324,23 @@ static int run_pipeline_fused(const ConfigList& cl, const nh_backflow_params& p,
   }
   return launch_combine(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev, sign,
                         logabs, flags, p.cancel_tau, nullptr, st);
+}
+
+// The plain form (FP32 CNN on CUDA cores, CUDA-core Pfaffian) runs the fused pipeline wherever it
+// applies; the other forms the unfused one.
+static bool use_fused(const nh_backflow_params& p) {
+  return p.cnn_mode == 0 && p.pf_mode == 0 && fused_ok(p);
+}
+
+static size_t amp_bytes(int items, const nh_backflow_params& p) {
+  return use_fused(p) ? fused_bytes((size_t)(items > 0 ? items : 1), p) : pipeline_bytes(items, p);
+}
+
+static int run_amplitudes(const ConfigList& cl, const nh_backflow_params& p, void* ws, int items,
+                          float* sign, double* logabs, int32_t* flags, cudaStream_t st) {
+  if (use_fused(p))
+    return run_pipeline_fused(cl, p, carve_fused(ws, (size_t)items, p), sign, logabs, flags, st);
+  return run_pipeline(cl, p, carve_pipeline(ws, items, p), sign, logabs, flags, st);
 }
 
 static int check_params(const nh_backflow_params* p) {
@@ -528,7 +549,7 @@ int nh_slogpf(const float* F, int n, int batch, double cond_tau, float* sign, do
 
 size_t nh_amplitude_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p) {
   if (!p) return 0;
-  return pipeline_bytes(batch * n_symm, *p);
+  return amp_bytes(batch * n_symm, *p);
 }
 
 int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_params* p,
@@ -541,9 +562,9 @@ int nh_amplitude(const int8_t* spins, int batch, int n_symm, const nh_backflow_p
   if (batch == 0) return NH_OK;
   const size_t need = nh_amplitude_workspace_bytes(batch, n_symm, p);
   if ((rc = check_workspace(workspace, workspace_bytes, need, "amplitude"))) return rc;
-  PipelineBuffers b = carve_pipeline(workspace, batch * n_symm, *p);
   ConfigList cl{spins, nullptr, nullptr, nullptr, nullptr, batch, n_symm};
-  return run_pipeline(cl, *p, b, sign, logabs, flags, static_cast<cudaStream_t>(stream));
+  return run_amplitudes(cl, *p, workspace, batch * n_symm, sign, logabs, flags,
+                        static_cast<cudaStream_t>(stream));
 }
 
 // ------------------------------------------------------------------ local energy
@@ -716,7 +737,7 @@ static MhLayout mh_layout(void* ws, int batch, int n_symm, const nh_backflow_par
   L.psign = reinterpret_cast<float*>(take((size_t)batch * 4));
   L.plogabs = reinterpret_cast<double*>(take((size_t)batch * 8));
   L.lqr = reinterpret_cast<float*>(take((size_t)batch * 4));
-  L.pipe = take(pipeline_bytes(batch * n_symm, *p));
+  L.pipe = take(amp_bytes(batch * n_symm, *p));
   L.bytes = off;
   return L;
 }
@@ -753,7 +774,6 @@ int nh_metropolis_steps_mixed(int8_t* spins, float* sign, double* logabs, int ba
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   MhLayout L = mh_layout(workspace, batch, n_symm, p);
   const int N = p->Lx * p->Ly;
-  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, *p);
   for (int t = 0; t < nsteps; ++t) {
     const int64_t step = step0 + t;
     if ((rc = launch_mh_propose(spins, batch, p->Lx, p->Ly, n_dirs, seed, step, L.valid, L.from,
@@ -763,7 +783,8 @@ int nh_metropolis_steps_mixed(int8_t* spins, float* sign, double* logabs, int ba
                              L.c_count, st)))
       return rc;
     ConfigList cl{spins, L.c_sample, L.c_from, L.c_to, L.c_count, batch, n_symm};
-    if ((rc = run_pipeline(cl, *p, b, L.psign, L.plogabs, nullptr, st))) return rc;
+    if ((rc = run_amplitudes(cl, *p, L.pipe, batch * n_symm, L.psign, L.plogabs, nullptr, st)))
+      return rc;
     if ((rc = launch_mh_accept(spins, sign, logabs, batch, N, L.c_sample, L.c_from, L.c_to,
                                L.c_count, L.psign, L.plogabs, nullptr, seed, step, accepted,
                                st)))
@@ -797,7 +818,6 @@ int nh_metropolis_steps_learned(int8_t* spins, float* sign, double* logabs, int 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   MhLayout L = mh_layout(workspace, batch, n_symm, p);
   const int N = p->Lx * p->Ly;
-  PipelineBuffers b = carve_pipeline(L.pipe, batch * n_symm, *p);
   for (int t = 0; t < nsteps; ++t) {
     const int64_t step = step0 + t;
     if ((rc = launch_prop_sample(spins, batch, *q, seed, step, L.valid, L.from, L.to, L.lqr, st)))
@@ -806,7 +826,8 @@ int nh_metropolis_steps_learned(int8_t* spins, float* sign, double* logabs, int 
                              L.c_count, st)))
       return rc;
     ConfigList cl{spins, L.c_sample, L.c_from, L.c_to, L.c_count, batch, n_symm};
-    if ((rc = run_pipeline(cl, *p, b, L.psign, L.plogabs, nullptr, st))) return rc;
+    if ((rc = run_amplitudes(cl, *p, L.pipe, batch * n_symm, L.psign, L.plogabs, nullptr, st)))
+      return rc;
     if ((rc = launch_mh_accept(spins, sign, logabs, batch, N, L.c_sample, L.c_from, L.c_to,
                                L.c_count, L.psign, L.plogabs, L.lqr, seed, step, accepted, st)))
       return rc;

@@ -355,6 +355,10 @@ struct FusedLaunch {
   int32_t* queue;
 };
 bool fused_supported(const nh_backflow_params& p);
+// The FP32 gather + Pfaffian with the item's rows copied into shared memory first (the gather
+// reads them there instead of from global memory per element); FP32, n <= 256, d % 4 == 0.
+bool staged_supported(const PfGatherArgs& g);
+int launch_pfaffian_staged(const PfGatherArgs& g, cudaStream_t st);
 int launch_pfaffian_fused(const FusedLaunch& f, cudaStream_t st);
 // Tensor-memory Pfaffian (one matrix per SM, trailing updates on tcgen05): mode 1 gathers from
 // g.Y / g.idx / g.Wt (FP32), mode 0 reads dense F (items, n, n) FP32.

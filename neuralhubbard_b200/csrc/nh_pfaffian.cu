@@ -207,16 +207,51 @@ __device__ void gather_lower(T* Lw, int n, const T* __restrict__ Y, const int32_
   }
 }
 
-// Mode 2 load phase of one item: the CNN of its configuration in shared memory, its occupied rows
-// Y and modes written to shared memory (write_occupied_rows, item sign to item_sign_out), then
-// the gather of the lower triangle from them.  Rows of the triangle that overlap Y (tail_row on)
-// are computed into registers first and stored after a barrier.
+// Load phase of modes 2 and 3: the item's occupied rows Y (n, D) and modes in shared memory
+// (mode 2: the CNN of its configuration in shared memory, write_occupied_rows, item sign to
+// item_sign_out; mode 3: copied from the global rows a.Y / a.idx of slot), then the gather of
+// the lower triangle from them.  Rows of the triangle that overlap Y (tail_row on) are computed
+// into registers first and stored after a barrier.
 constexpr int kTailRegs = 16;
 
 template <int D>
-__device__ void features_and_gather(const PfArgs& a, int item, float* Lw, unsigned char* smem) {
-  const int n = a.n, N = a.Lx * a.Ly, C = a.C, M2 = 2 * N, NS = N + 1;
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+__device__ void features_to_smem(const PfArgs& a, int item, unsigned char* smem, float* Ys,
+                                 int* ids);
+template <int D>
+__device__ void gather_from_rows(const PfArgs& a, float* Lw, const float* Ys, const int* ids);
+
+template <int D>
+__device__ void rows_and_gather(const PfArgs& a, int item, int slot, float* Lw,
+                                unsigned char* smem) {
+  const int n = a.n;
+  const int tid = threadIdx.x;
+  float* Ys = reinterpret_cast<float*>(smem + a.y_off);
+  int* ids = reinterpret_cast<int*>(smem + a.idx_off);
+  if (a.mode == 3) {
+    const float4* src = reinterpret_cast<const float4*>(static_cast<const float*>(a.Y) +
+                                                        (size_t)slot * n * D);
+    const int nv = n * D / 4;
+    for (int v0 = tid; v0 < nv; v0 += 4 * kNumThreads) {
+      float4 buf[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (v0 + u * kNumThreads < nv) buf[u] = __ldg(src + v0 + u * kNumThreads);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (v0 + u * kNumThreads < nv) reinterpret_cast<float4*>(Ys)[v0 + u * kNumThreads] = buf[u];
+    }
+    for (int p = tid; p < n; p += kNumThreads) ids[p] = __ldg(a.idx + (size_t)slot * n + p);
+    __syncthreads();
+  } else {
+    features_to_smem<D>(a, item, smem, Ys, ids);
+  }
+  gather_from_rows<D>(a, Lw, Ys, ids);
+}
+
+template <int D>
+__device__ void features_to_smem(const PfArgs& a, int item, unsigned char* smem, float* Ys,
+                                 int* ids) {
+  const int N = a.Lx * a.Ly, C = a.C, M2 = 2 * N, NS = N + 1;
   const int G = a.cl.G;
   const int c = item / G, g = item - c * G;
   const int smp = a.cl.sample ? a.cl.sample[c] : c;
@@ -235,14 +270,19 @@ __device__ void features_and_gather(const PfArgs& a, int item, float* Lw, unsign
   float* bsm = wsm + C * C * 9;
   const float* in = cnn_layers<float>(a.cnn_w, a.cnn_b, a.Lx, a.Ly, C, a.layers, base, fr, to,
                                       g, actA, actB, wsm, bsm, simg);
-  float* Ys = reinterpret_cast<float*>(smem + a.y_off);
-  int* ids = reinterpret_cast<int*>(smem + a.idx_off);
   const int d = C / 2;
-  write_occupied_rows(simg, occl, wbuf, N, n, d, g, a.Lx, a.Ly, Ys, ids, a.item_sign_out + item,
+  write_occupied_rows(simg, occl, wbuf, N, a.n, d, g, a.Lx, a.Ly, Ys, ids,
+                      a.item_sign_out + item,
                       [&](int sg, int aa, int site) { return in[(sg * d + aa) * NS + site]; });
   __syncthreads();
+}
+
+template <int D>
+__device__ void gather_from_rows(const PfArgs& a, float* Lw, const float* Ys, const int* ids) {
+  const int n = a.n, N = a.Lx * a.Ly;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const float* Wt = static_cast<const float*>(a.Wt);
-  // rows below tail_row: straight into the triangle, warp <-> row, lane <-> column
+  // rows below tail_row: straight into the triangle, warp <-> row, lane <-> two columns in flight
   for (int p = wid; p < a.tail_row; p += kNumThreads / 32) {
     float yp[D];
 #pragma unroll
@@ -255,7 +295,14 @@ __device__ void features_and_gather(const PfArgs& a, int item, float* Lw, unsign
     }
     const int mp = ids[p];
     float* row = Lw + ((p * (p - 1)) >> 1);
-    for (int q = lane; q < p; q += 32) row[q] = pair_smem<D>(yp, mp, Ys, ids, q, N, a.Lx, a.Ly, Wt);
+    int q = lane;
+    for (; q + 32 < p; q += 64) {
+      const float v0 = pair_smem<D>(yp, mp, Ys, ids, q, N, a.Lx, a.Ly, Wt);
+      const float v1 = pair_smem<D>(yp, mp, Ys, ids, q + 32, N, a.Lx, a.Ly, Wt);
+      row[q] = v0;
+      row[q + 32] = v1;
+    }
+    if (q < p) row[q] = pair_smem<D>(yp, mp, Ys, ids, q, N, a.Lx, a.Ly, Wt);
   }
   if (a.tail_row < n) {
     // rows tail_row .. n-1 (E elements, at most kTailRegs per thread) through registers
@@ -340,9 +387,7 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
     const int item = a.slot_item ? a.slot_item[slot] : slot;
     __syncthreads();
     if constexpr (sizeof(T) == 4 && THREADS == kNumThreads && D % 4 == 0) {
-      if (a.mode == 2) {
-        features_and_gather<D>(a, item, Lw, smem_raw);
-      }
+      if (a.mode >= 2) rows_and_gather<D>(a, item, slot, Lw, smem_raw);
     }
     if (a.mode == 0) {
       const float* F = a.F + (size_t)item * n * n;
@@ -1399,8 +1444,8 @@ int launch_fused_nb(PfArgs a, cudaStream_t st) {
   const int n = a.n, N = a.Lx * a.Ly;
   constexpr int WARPS = kWarps;
   const size_t pf = pf_smem<float, NB>(n);
-  size_t cnn_end;
-  const size_t act_end = cnn_phase_layout(N, a.C, a.Lx, &cnn_end);
+  size_t cnn_end = 0, act_end = 0;  // mode 3 (rows copied from global memory): no CNN phase
+  if (a.mode == 2) act_end = cnn_phase_layout(N, a.C, a.Lx, &cnn_end);
   const size_t tri_pad = ((size_t)n * (n - 1) / 2 + 3) & ~(size_t)3;
   const size_t tri_bytes = 4 * tri_pad, y_bytes = 4 * (size_t)n * D;
   const size_t two_cta = 113 * 1024;
@@ -1507,6 +1552,41 @@ bool fused_supported(const nh_backflow_params& p) {
   const int n = p.n_up + p.n_dn, N = p.Lx * p.Ly, d = p.channels / 2;
   return p.net == NH_NET_CNN && n <= kNumThreads && n % 2 == 0 && N % 2 == 0 &&
          p.channels % 16 == 0 && p.channels <= 64 && (d == 8 || d == 16 || d == 32);
+}
+
+bool staged_supported(const PfGatherArgs& g) {
+  return !g.fp64 && g.n <= kNumThreads && g.n % 2 == 0 && g.d % 4 == 0 && g.d <= 32 && !g.tri;
+}
+
+int launch_pfaffian_staged(const PfGatherArgs& g, cudaStream_t st) {
+  PfArgs a{};
+  a.n = g.n;
+  a.mode = 3;
+  a.Y = g.Y;
+  a.idx = g.idx;
+  a.Wt = g.Wt;
+  a.Lx = g.Lx;
+  a.Ly = g.Ly;
+  a.count_dev = g.count_dev;
+  a.count_mult = g.count_mult;
+  a.n_slots = g.n_slots;
+  a.slot_item = g.slot_item;
+  a.item_sign = g.item_sign;
+  a.sign = g.sign;
+  a.logabs = g.logabs;
+  a.flags = g.flags;
+  a.cond_tau = g.cond_tau;
+  a.flag_or = g.flag_or;
+  a.perm = g.perm;
+  a.refine_tau = g.refine_tau;
+  a.ratio = g.ratio;
+  const bool nb8 = pf_smem<float, 8>(a.n) <= 113 * 1024;
+  switch (g.d) {
+    case 8: return nb8 ? launch_fused_nb<8, 8>(a, st) : launch_fused_nb<4, 8>(a, st);
+    case 16: return nb8 ? launch_fused_nb<8, 16>(a, st) : launch_fused_nb<4, 16>(a, st);
+    case 32: return nb8 ? launch_fused_nb<8, 32>(a, st) : launch_fused_nb<4, 32>(a, st);
+    default: return fail(NH_ERR_UNSUPPORTED, "staged Pfaffian: d=%d", g.d);
+  }
 }
 
 int launch_pfaffian_fused(const FusedLaunch& f, cudaStream_t st) {

@@ -269,7 +269,7 @@ def test_learned_sampler_against_plain_8x8():
     state = nh.Variational(nh.PfaffianBackflow(L, L, ne, ne, params=params), symm=True)
     B = 1024
     plain = nh.ParticleHop(state, B, n_neighbor=(1, 2), seed=1)
-    plain.run(400)
+    plain.run(1500)  # equilibrate: both samplers must start from |psi|^2 for the energy A/B
     snaps = []
     for _ in range(16):
         plain.run(1)
@@ -280,10 +280,10 @@ def test_learned_sampler_against_plain_8x8():
     q.train(rec, 300, batch=512, lr=3e-3)
     learned = nh.LearnedHop(state, B, q, initial_spins=start, seed=4)
     a_p0, a_l0 = plain.accepted.sum().item(), learned.accepted.sum().item()
-    plain.run(300)
-    learned.run(300)
-    acc_p = (plain.accepted.sum().item() - a_p0) / (B * 300)
-    acc_l = (learned.accepted.sum().item() - a_l0) / (B * 300)
+    plain.run(600)
+    learned.run(600)
+    acc_p = (plain.accepted.sum().item() - a_p0) / (B * 600)
+    acc_l = (learned.accepted.sum().item() - a_l0) / (B * 600)
     assert acc_l > 1.2 * acc_p, (acc_l, acc_p)
     H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2])
     e = []
