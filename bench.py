@@ -825,7 +825,8 @@ def run_ours(args) -> None:
         amps_per_launch = BATCH * IMAGES * args.steps / launches
         flop = {"cnn": CNN_FLOP, "cnn_tc": CNN_FLOP,
                 "pfaffian": PFAFFIAN_FLOP + GATHER_FLOP,
-                "pfaffian_tc": PFAFFIAN_FLOP + GATHER_FLOP}.get(dom, 0.0)
+                "pfaffian_tc": PFAFFIAN_FLOP + GATHER_FLOP,
+                "fused": CNN_FLOP + PFAFFIAN_FLOP + GATHER_FLOP}.get(dom, 0.0)
         achieved = flop * amps_per_launch / per_launch_s / 1e12
         tb = TRAFFIC_BYTES.get(dom)
         roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": bf16,

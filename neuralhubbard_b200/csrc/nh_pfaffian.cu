@@ -400,6 +400,9 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
       gather_lower<T, D, WARPS>(Lw, n, Ybase + (size_t)slot * n * D, a.idx + (size_t)slot * n,
                                 Wt, a.Lx, a.Ly);
     }
+    // Modes 2 and 3: the rows in shared memory can overlap the factorisation's scratch (misc
+    // among it), so every warp's gather reads end before the first scratch write.
+    if (a.mode >= 2) __syncthreads();
     if (tid == 0) misc[0] = 0;
     __syncthreads();
 
@@ -1491,7 +1494,7 @@ int launch_fused_nb(PfArgs a, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(int32_t), st);
     if (e != cudaSuccess) return check_cuda(e, "fused amplitude: clear work counter");
   }
-  ProfScope prof_scope(NH_K_FUSED, st);
+  ProfScope prof_scope(a.mode == 2 ? NH_K_FUSED : NH_K_PFAFFIAN, st);
   pfaffian_kernel<float, NB, D, kNumThreads><<<grid, kNumThreads, smem, st>>>(a);
   return check_launch("pfaffian_kernel (fused features)");
 }
