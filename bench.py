@@ -948,6 +948,9 @@ def run_reference(args) -> None:
 #   resconv_tc         residual network (16 blocks x 64 channels) on tcgen05, 16x16, 64 x 8 images
 #   resconv            the same network on CUDA cores (FP32)
 #   refine             16x16 projected amplitudes, 512 x 8 images, every image refined in FP64
+#   amplitude          16x16 projected amplitudes, 1024 x 8 images, tcgen05 CNN + staged FP32
+#                      Pfaffian + default refinement (the benchmark's chosen form)
+#   amplitude_plain    the same on the plain form (fused FP32 CNN + Pfaffian kernel)
 
 def _model(L, cnn_mode=0):
     import neuralhubbard_b200 as nh
@@ -1083,10 +1086,31 @@ def case_refine(repeat):
         state(s)
 
 
+def _amplitude(repeat, cnn_mode):
+    import torch
+
+    import neuralhubbard_b200 as nh
+
+    model, ne = _model(16, cnn_mode=cnn_mode)
+    state = nh.Variational(model, symm=True)
+    s = torch.from_numpy(nh.random_spins(np.random.default_rng(9), 1024, 256, ne, ne)).cuda()
+    for _ in range(repeat):
+        state(s)
+
+
+def case_amplitude(repeat):
+    _amplitude(repeat, 2)
+
+
+def case_amplitude_plain(repeat):
+    _amplitude(repeat, 0)
+
+
 CASES = {"pairing": case_pairing, "hops": case_hops, "eloc": case_eloc,
          "proposal_sample": case_proposal_sample, "proposal_backward": case_proposal_backward,
          "resconv_tc": case_resconv_tc, "resconv": case_resconv,
-         "refine": case_refine}
+         "refine": case_refine, "amplitude": case_amplitude,
+         "amplitude_plain": case_amplitude_plain}
 
 
 
@@ -1097,7 +1121,7 @@ def main():
     ap.add_argument("--profile-case", default=None,
                     help="run one fixed profiling workload instead of the benchmark (cases: "
                          "pairing, hops, eloc, proposal_sample, proposal_backward, resconv_tc, "
-                         "resconv, refine)")
+                         "resconv, refine, amplitude, amplitude_plain)")
     ap.add_argument("--repeat", type=int, default=2, help="repetitions of --profile-case")
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
