@@ -255,7 +255,8 @@ def run_chains(smp, steps, st):
 def measure_sampling(args, dev, st, seed) -> dict:
     """Effective samples/s of the plain form (FP32 CNN, uniform-hop sampler) and the chosen form
     (tcgen05 BF16x3 CNN, learned proposal trained on 2^20 records of plain chains), plus the
-    chosen amplitudes under the uniform-hop sampler.  All chains start from the same
+    chosen amplitudes under the uniform-hop sampler and under the reference's MixSampler (hop and
+    site-exchange chains, half each).  All chains start from the same
     configurations, equilibrated by ``burn`` plain steps; tau_int is that of the log|psi| series
     over the ``steps`` measured steps; energies per site from the final configurations."""
     import torch
@@ -309,15 +310,26 @@ def measure_sampling(args, dev, st, seed) -> dict:
                                                          initial_spins=s, seed=seed + 6)),
             ("chosen_uniform_hop", "chosen",
              lambda s: nh.ParticleHop(states["chosen"], B, n_neighbor=(1, 2), initial_spins=s,
-                                      seed=seed + 7))]
+                                      seed=seed + 7)),
+            # the reference's own sampler: MixSampler of hop and site-exchange chains, half each
+            ("chosen_mix", "chosen",
+             lambda s: nh.MixSampler([nh.ParticleHop(states["chosen"], B // 2, n_neighbor=(1, 2)),
+                                      nh.SiteExchange(states["chosen"], B - B // 2,
+                                                      n_neighbor=(1, 2))],
+                                     initial_spins=s, seed=seed + 8))]
     for name, form, make in runs:
         smp = make(start)
         series, ms, acc = run_chains(smp, steps, st)
-        tau = stats.tau_int(series)
+        te = stats.tau_int_error(series)
+        tau = te["tau"]
+        err = te["err_groups"] if te["err_groups"] is not None else te["err_sokal"]
+        rate = stats.effective_rate(B, steps, tau, ms / 1e3)
         e = H.Oloc(states[form], nh.Samples(smp.spins[:ne].contiguous(), smp.psi[:ne]))
         e = e.cpu().numpy() / N_SITES
-        out[name] = {"acceptance": acc, "tau_int_logpsi": tau, "ms_per_step": ms / steps,
-                     "effective_samples_per_s": stats.effective_rate(B, steps, tau, ms / 1e3),
+        out[name] = {"acceptance": acc, "tau_int_logpsi": tau, "tau_int_logpsi_err": err,
+                     "tau_int_logpsi_err_sokal": te["err_sokal"], "tau_window": te["window"],
+                     "ms_per_step": ms / steps, "effective_samples_per_s": rate,
+                     "effective_samples_per_s_err": rate * err / tau,
                      "energy_per_site": float(e.mean()),
                      "energy_per_site_err": float(e.std(ddof=1) / np.sqrt(ne))}
         del smp
@@ -330,11 +342,15 @@ def measure_sampling(args, dev, st, seed) -> dict:
                               / out["plain"]["effective_samples_per_s"])
     out["chosen_uniform_hop_vs_plain"] = (out["chosen_uniform_hop"]["effective_samples_per_s"]
                                           / out["plain"]["effective_samples_per_s"])
+    out["chosen_mix_vs_plain"] = (out["chosen_mix"]["effective_samples_per_s"]
+                                  / out["plain"]["effective_samples_per_s"])
     out["setup"] = {"chains": B, "burn_in_steps": burn, "burn_in_seconds": t_burn,
                     "measured_steps": steps,
                     "start": "all runs from the same configurations after the burn-in",
                     "tau_convention": "Sokal tau = 1/2 + sum rho (window c = 5); effective = "
-                                      "B steps / (2 tau seconds)",
+                                      "B steps / (2 tau seconds); tau error = spread of tau over "
+                                      "8 disjoint sets of chains / sqrt(8) (Sokal's variance "
+                                      "formula beside it)",
                     "energy_samples": ne, "seconds_are": "CUDA-event time of the measured steps"}
     return out
 
@@ -362,7 +378,7 @@ def measure_local_energy(args, dev, st) -> dict:
                                                  nek)).to(dev)
         psi = state(spins)
         sub = nh.Samples(spins[:256].contiguous(), psi[:256])
-        chunk = H.autotune(state, sub, candidates=(4096, 16384, 65536), repeats=1)
+        chunk = H.autotune(state, sub, candidates=(0, 4096, 16384, 65536), repeats=1)
         counts = H.hop_list(spins, Lk, Lk)[0]
         n_conn = int(counts.sum().item())
         samples = nh.Samples(spins, psi)

@@ -615,10 +615,11 @@ static ElocLayout eloc_layout(void* ws, int batch, int n_symm, int chunk,
   return L;
 }
 
-// chunk_configs <= 0 selects the persistent path where the network supports it.
+// chunk_configs <= 0 selects the persistent path where the form runs the fused pipeline (plain
+// FP32 CNN and CUDA-core Pfaffian); the tensor-core forms keep their own kernels, chunked.
 static int eloc_chunk(int chunk_configs, const nh_backflow_params* p) {
   if (chunk_configs > 0) return chunk_configs;
-  return fused_ok(*p) ? 0 : kDefaultChunk;
+  return use_fused(*p) ? 0 : kDefaultChunk;
 }
 
 size_t nh_local_energy_workspace_bytes(int batch, int n_symm, int chunk_configs,

@@ -28,15 +28,40 @@ def autocorrelation(x: np.ndarray) -> np.ndarray:
     return acov / acov[0]
 
 
-def tau_int(x: np.ndarray, c: float = 5.0) -> float:
-    """Integrated autocorrelation time tau = 1/2 + sum_{t=1}^{W} rho(t) with Sokal's window."""
+def tau_int_window(x: np.ndarray, c: float = 5.0):
+    """(tau, W): tau = 1/2 + sum_{t=1}^{W} rho(t) and Sokal's window W (the smallest W with
+    W >= c tau(W))."""
     rho = autocorrelation(x)
     tau = 0.5
+    W = 0
     for W in range(1, len(rho)):
         tau += rho[W]
         if W >= c * tau:
             break
-    return float(max(tau, 0.5))
+    return float(max(tau, 0.5)), int(W)
+
+
+def tau_int(x: np.ndarray, c: float = 5.0) -> float:
+    """Integrated autocorrelation time tau = 1/2 + sum_{t=1}^{W} rho(t) with Sokal's window."""
+    return tau_int_window(x, c)[0]
+
+
+def tau_int_error(x: np.ndarray, c: float = 5.0, groups: int = 8) -> dict:
+    """tau_int of a (T, B) chain series with two error bars: Sokal's variance estimate
+    var(tau) = 2 (2W + 1) / (T B) tau^2 (independent chains averaged), and the spread of tau over
+    ``groups`` disjoint sets of chains divided by sqrt(groups) (empirical; needs B >= 2 groups)."""
+    x = np.asarray(x, np.float64)
+    if x.ndim == 1:
+        x = x[:, None]
+    T, B = x.shape
+    tau, W = tau_int_window(x, c)
+    out = {"tau": tau, "window": W, "err_sokal": float(np.sqrt(2.0 * (2 * W + 1) / (T * B)) * tau)}
+    if B >= 2 * groups:
+        taus = [tau_int(x[:, g::groups], c) for g in range(groups)]
+        out["err_groups"] = float(np.std(taus, ddof=1) / np.sqrt(groups))
+    else:
+        out["err_groups"] = None
+    return out
 
 
 def effective_rate(n_chains: int, n_steps: int, tau: float, seconds: float) -> float:

@@ -160,6 +160,28 @@ def test_tau_int_matches_oracle_and_ar1():
     assert stats.effective_rate(64, 4000, 0.5, 2.0) == 64 * 4000 / 2.0
 
 
+def test_tau_int_error_bars_cover_ar1():
+    """The error bars of tau_int: across 12 seeds of an AR(1) ensemble the estimate lies within
+    3 (group-spread) error bars of the closed form, with the window's small downward bias
+    included, and the two error estimates agree within a factor of 4."""
+    from neuralhubbard_b200 import stats
+
+    phi, T, B = 0.8, 2000, 128
+    exact = (1 + phi) / (2 * (1 - phi))
+    for seed in range(12):
+        rng = np.random.default_rng(100 + seed)
+        x = np.zeros((T, B))
+        e = rng.normal(size=(T, B))
+        for t in range(1, T):
+            x[t] = phi * x[t - 1] + e[t]
+        te = stats.tau_int_error(x)
+        assert te["tau"] == stats.tau_int(x)
+        assert te["window"] >= 5 * te["tau"]
+        assert abs(te["tau"] - exact) < 3 * te["err_groups"] + 0.15, (seed, te)
+        assert 0.25 < te["err_groups"] / te["err_sokal"] < 4.0, te
+    assert stats.tau_int_error(np.zeros((100, 4)))["err_groups"] is None
+
+
 def test_residual_network_argument_checks():
     """Packing sizes and the parameter checks of the residual network (net = NH_NET_RESCONV),
     all decided before any device work."""
