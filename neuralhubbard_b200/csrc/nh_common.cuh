@@ -142,14 +142,28 @@ __device__ __forceinline__ int block_scan(int v, int* warp_buf, int* total) {
   return base + x - v;
 }
 
+// Shared-memory rows of W values whose 16-byte chunks are XOR-swizzled by a row key, so that
+// eight consecutive rows reading the same chunk (one quarter-warp of 16-byte loads) hit eight
+// different groups of four banks: element a of row r sits at swz_index(r, a).  K = W * size / 16
+// chunks per row (1, 2, 4 or 8); the key is ((r K) >> 3) & (K - 1), zero for one-chunk rows.
+__host__ __device__ __forceinline__ int swz_key(int r, int K) {
+  return K > 1 ? ((r * K) >> 3) & (K - 1) : 0;
+}
+template <typename T, int W>
+__host__ __device__ __forceinline__ int swz_index(int r, int a) {
+  constexpr int E = 16 / sizeof(T), K = W / E;
+  return r * W + (((a / E) ^ swz_key(r, K)) * E) + (a % E);
+}
+
 // Mode-1 output of the backflow networks for one item, by a kNumThreads block: the ascending
 // occupied modes of the image configuration simg (+-1, 2N), the rows Y[p, a] = feat(spin, a,
 // site) of those modes (p < n), their mode indices, and the item sign eta_g(s) (-1)^(k(k-1)/2)
 // (0 for a wrong particle number k != n).  occl: 2N ints; wbuf: 4 Lx + 32 ints.
+// swizzle: rows in the chunk-swizzled layout of swz_index (shared-memory destinations).
 template <typename T, typename Feat>
 __device__ void write_occupied_rows(const int* simg, int* occl, int* wbuf, int N, int n, int d,
                                     int g, int Lx, int Ly, T* Ydst, int32_t* idst,
-                                    float* sign_dst, Feat feat) {
+                                    float* sign_dst, Feat feat, bool swizzle = false) {
   const int tid = threadIdx.x, M2 = 2 * N;
   const int per = (M2 + kNumThreads - 1) / kNumThreads;
   const int m0 = tid * per;
@@ -160,11 +174,13 @@ __device__ void write_occupied_rows(const int* simg, int* occl, int* wbuf, int N
   for (int m = m0; m < m0 + per && m < M2; ++m)
     if (simg[m] > 0) occl[pos++] = m;
   __syncthreads();
+  const int E = 16 / (int)sizeof(T), K = d / E;  // swizzled rows: K 16-byte chunks of E values
   for (int o = tid; o < n * d; o += kNumThreads) {
     const int p = o / d, aa = o - p * d;
     const int m = occl[p < total ? p : 0];
     const int sg = m >= N ? 1 : 0;
-    Ydst[o] = feat(sg, aa, m - sg * N);
+    const int dst = swizzle ? p * d + ((aa / E) ^ swz_key(p, K)) * E + aa % E : o;
+    Ydst[dst] = feat(sg, aa, m - sg * N);
   }
   for (int p = tid; p < n; p += kNumThreads) idst[p] = occl[p < total ? p : 0];
   // eta_g from per-row occupation counts (closed form of the inversion parity).

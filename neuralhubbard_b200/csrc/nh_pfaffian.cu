@@ -117,27 +117,30 @@ __host__ __device__ inline size_t cnn_phase_layout(int N, int C, int Lx, size_t*
   return act_end;
 }
 
-// F[p][q] (p > q) of the item from occupied rows Y (n, D) and modes in shared memory, the same
-// arithmetic as pair_value: sum_a (Y[p, a] Y[q, a]) Wt[2 s_p + s_q, r(p, q), a] in order of a.
+// A mode m (spin s = m >= N, site x Ly + y) packed as s << 16 | x << 8 | y for the gather from
+// shared memory (no division per element).
+__device__ __forceinline__ int pack_mode(int m, int N, int Ly) {
+  const int s = m >= N ? 1 : 0, site = m - s * N, x = site / Ly;
+  return (s << 16) | (x << 8) | (site - x * Ly);
+}
+
+// F[p][q] (p > q) of the item from occupied rows Y (n, D, chunk-swizzled: swz_index) and packed
+// modes (pack_mode) in shared memory, the same arithmetic as pair_value:
+// sum_a (Y[p, a] Y[q, a]) Wt[2 s_p + s_q, r(p, q), a] in order of a.
 template <int D>
-__device__ __forceinline__ float pair_smem(const float* yp, int mp, const float* __restrict__ Ys,
+__device__ __forceinline__ float pair_smem(const float* yp, int cp, const float* __restrict__ Ys,
                                            const int* __restrict__ ids, int q, int N, int Lx,
                                            int Ly, const float* __restrict__ Wt) {
-  const int sp = mp >= N ? 1 : 0, sitep = mp - sp * N;
-  const int xp = sitep / Ly, ypos = sitep - xp * Ly;
-  const int mq = ids[q];
-  const int sq = mq >= N ? 1 : 0, siteq = mq - sq * N;
-  const int xq = siteq / Ly, yq = siteq - xq * Ly;
-  int dx = xp - xq, dy = ypos - yq;
+  const int cq = ids[q];
+  int dx = ((cp >> 8) & 0xff) - ((cq >> 8) & 0xff), dy = (cp & 0xff) - (cq & 0xff);
   dx += dx < 0 ? Lx : 0;
   dy += dy < 0 ? Ly : 0;
-  const float* wrow = Wt + ((size_t)(2 * sp + sq) * N + dx * Ly + dy) * D;
-  const float* yq_row = Ys + q * D;
+  const float* wrow = Wt + ((size_t)(2 * (cp >> 16) + (cq >> 16)) * N + dx * Ly + dy) * D;
   float acc = 0.0f;
 #pragma unroll
   for (int a0 = 0; a0 < D; a0 += 4) {
     const float4 w = __ldg(reinterpret_cast<const float4*>(wrow + a0));
-    const float4 v = *reinterpret_cast<const float4*>(yq_row + a0);
+    const float4 v = *reinterpret_cast<const float4*>(Ys + swz_index<float, D>(q, a0));
     acc = fmaf(yp[a0] * v.x, w.x, acc);
     acc = fmaf(yp[a0 + 1] * v.y, w.y, acc);
     acc = fmaf(yp[a0 + 2] * v.z, w.z, acc);
@@ -207,7 +210,7 @@ __device__ void gather_lower(T* Lw, int n, const T* __restrict__ Y, const int32_
   }
 }
 
-// Load phase of modes 2 and 3: the item's occupied rows Y (n, D) and modes in shared memory
+// Load phase of modes 2 and 3: the item's occupied rows Y (n, D) and packed modes in shared memory
 // (mode 2: the CNN of its configuration in shared memory, write_occupied_rows, item sign to
 // item_sign_out; mode 3: copied from the global rows a.Y / a.idx of slot), then the gather of
 // the lower triangle from them.  Rows of the triangle that overlap Y (tail_row on) are computed
@@ -230,17 +233,22 @@ __device__ void rows_and_gather(const PfArgs& a, int item, int slot, float* Lw,
   if (a.mode == 3) {
     const float4* src = reinterpret_cast<const float4*>(static_cast<const float*>(a.Y) +
                                                         (size_t)slot * n * D);
-    const int nv = n * D / 4;
+    constexpr int K = D / 4;  // 16-byte chunks per row, stored swizzled (swz_index)
+    const int nv = n * K;
     for (int v0 = tid; v0 < nv; v0 += 4 * kNumThreads) {
       float4 buf[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u)
         if (v0 + u * kNumThreads < nv) buf[u] = __ldg(src + v0 + u * kNumThreads);
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (v0 + u * kNumThreads < nv) reinterpret_cast<float4*>(Ys)[v0 + u * kNumThreads] = buf[u];
+      for (int u = 0; u < 4; ++u) {
+        const int v = v0 + u * kNumThreads, row = v / K;
+        if (v < nv) reinterpret_cast<float4*>(Ys)[row * K + ((v % K) ^ swz_key(row, K))] = buf[u];
+      }
     }
-    for (int p = tid; p < n; p += kNumThreads) ids[p] = __ldg(a.idx + (size_t)slot * n + p);
+    const int N = a.Lx * a.Ly;
+    for (int p = tid; p < n; p += kNumThreads)
+      ids[p] = pack_mode(__ldg(a.idx + (size_t)slot * n + p), N, a.Ly);
     __syncthreads();
   } else {
     features_to_smem<D>(a, item, smem, Ys, ids);
@@ -273,7 +281,10 @@ __device__ void features_to_smem(const PfArgs& a, int item, unsigned char* smem,
   const int d = C / 2;
   write_occupied_rows(simg, occl, wbuf, N, a.n, d, g, a.Lx, a.Ly, Ys, ids,
                       a.item_sign_out + item,
-                      [&](int sg, int aa, int site) { return in[(sg * d + aa) * NS + site]; });
+                      [&](int sg, int aa, int site) { return in[(sg * d + aa) * NS + site]; },
+                      true);
+  __syncthreads();
+  for (int p = threadIdx.x; p < a.n; p += kNumThreads) ids[p] = pack_mode(ids[p], N, a.Ly);
   __syncthreads();
 }
 
@@ -287,7 +298,7 @@ __device__ void gather_from_rows(const PfArgs& a, float* Lw, const float* Ys, co
     float yp[D];
 #pragma unroll
     for (int a0 = 0; a0 < D; a0 += 4) {
-      const float4 v = *reinterpret_cast<const float4*>(Ys + p * D + a0);
+      const float4 v = *reinterpret_cast<const float4*>(Ys + swz_index<float, D>(p, a0));
       yp[a0] = v.x;
       yp[a0 + 1] = v.y;
       yp[a0 + 2] = v.z;
@@ -320,7 +331,7 @@ __device__ void gather_from_rows(const PfArgs& a, float* Lw, const float* Ys, co
         float yp[D];
 #pragma unroll
         for (int a0 = 0; a0 < D; a0 += 4) {
-          const float4 y4 = *reinterpret_cast<const float4*>(Ys + p * D + a0);
+          const float4 y4 = *reinterpret_cast<const float4*>(Ys + swz_index<float, D>(p, a0));
           yp[a0] = y4.x;
           yp[a0 + 1] = y4.y;
           yp[a0 + 2] = y4.z;
@@ -367,9 +378,13 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
   constexpr int kValSlots = sizeof(T) == 4 ? 0 : WARPS;
   T* rval = Vs + n * NB;                 // (warps, FP64 only) candidate signed value
   T* pivs = rval + kValSlots;            // (n / 2) signed pivots, multiplied at the end
-  float* rkey = reinterpret_cast<float*>(pivs + ((n / 2 + 3) & ~3));  // (warps) candidate key
-  int* rt = reinterpret_cast<int*>(rkey + WARPS);  // (warps) candidate row; later ballot counts
-  int* rlog = rt + WARPS;                          // (warps) candidate logical label
+  float* rkey = reinterpret_cast<float*>(pivs + ((n / 2 + 3) & ~3));
+  int* rt = reinterpret_cast<int*>(rkey + WARPS);  // (warps) trailing update: ballot counts
+  int* rlog = rt + WARPS;
+  // (warps) packed pivot candidates over rkey and rt: |c| key + 1 (bits 63..32), 0xFFFF - row
+  // (31..16), sign of c (15), logical label (14..0): the largest word is the largest |c|, ties
+  // to the lowest row.
+  unsigned long long* cand = reinterpret_cast<unsigned long long*>(rkey);
   int* alist = rlog + WARPS;                       // (n) active physical rows
   int* misc = alist + n;                            // [0] physical row of logical k, [1] item
 
@@ -427,12 +442,12 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
           const bool act = my_log > k;
           if (act) {
             c = aval(Lw, tid, ck);
-            if (j > 0) {  // row ck's panel values: 16-byte loads (rows are NB * sizeof(T) apart)
+            if (j > 0) {  // row ck's panel values: 16-byte loads (chunk-swizzled rows, swz_index)
               T vr[NB], ur[NB];
 #pragma unroll
               for (int q = 0; q < NB; q += Vec<T>::k) {
-                lds16(Vs + ck * NB + q, vr + q);
-                lds16(Us + ck * NB + q, ur + q);
+                lds16(Vs + swz_index<T, NB>(ck, q), vr + q);
+                lds16(Us + swz_index<T, NB>(ck, q), ur + q);
               }
 #pragma unroll
               for (int p = 0; p < NB; ++p)
@@ -447,40 +462,28 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
           const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
           const unsigned hit = __ballot_sync(0xffffffffu, key == kmax);
           if (lane == __ffs(hit) - 1) {
-            rkey[wid] = kmax ? __uint_as_float(kmax - 1u) : -1.0f;
-            rt[wid] = tid;
-            if constexpr (sizeof(T) == 4)  // FP32: |c| is the key, the sign rides in bit 31
-              rlog[wid] = my_log | (signbit(c) ? (int)0x80000000 : 0);
-            else {
-              rval[wid] = c;
-              rlog[wid] = my_log;
-            }
+            const unsigned lo = ((0xFFFFu - (unsigned)tid) << 16) |
+                                (signbit(c) ? 0x8000u : 0u) | ((unsigned)my_log & 0x7FFFu);
+            cand[wid] = ((unsigned long long)kmax << 32) | lo;
+            if constexpr (sizeof(T) == 8) rval[wid] = c;  // FP64 keeps the signed value
           }
           __syncthreads();  // (1) pivot candidates
-          float kw[WARPS];
+          unsigned long long best = 0;
 #pragma unroll
-          for (int w = 0; w < WARPS; w += 4) {
-            const float4 q4 = *reinterpret_cast<const float4*>(rkey + w);
-            kw[w] = q4.x;
-            kw[w + 1] = q4.y;
-            kw[w + 2] = q4.z;
-            kw[w + 3] = q4.w;
+          for (int w = 0; w < WARPS; w += 2) {
+            const ulonglong2 q2 = *reinterpret_cast<const ulonglong2*>(cand + w);
+            best = q2.x > best ? q2.x : best;
+            best = q2.y > best ? q2.y : best;
           }
-
-          float bk = kw[0];
-#pragma unroll
-          for (int w = 1; w < WARPS; ++w) bk = fmaxf(bk, kw[w]);
-          int w0 = WARPS - 1;
-#pragma unroll
-          for (int w = WARPS - 2; w >= 0; --w) w0 = kw[w] == bk ? w : w0;
-          const int r = rt[w0];
-          const int lw = rlog[w0];
-          const int lr = lw & 0x7FFFFFFF;
+          const unsigned kbest = (unsigned)(best >> 32);
+          const float bk = kbest ? __uint_as_float(kbest - 1u) : -1.0f;
+          const int r = 0xFFFF - (int)((best >> 16) & 0xFFFFu);
+          const int lr = (int)(best & 0x7FFFu);
           T cr;
           if constexpr (sizeof(T) == 4)
-            cr = lw < 0 ? -bk : bk;  // a NaN candidate comes back as an infinite pivot
+            cr = (best & 0x8000u) ? -bk : bk;  // a NaN candidate comes back as an infinite pivot
           else
-            cr = rval[w0];
+            cr = rval[r >> 5];
           if (!(bk > 0.0f)) {
             zero = true;  // exactly singular (or empty) column: pf = 0
           } else {
@@ -497,8 +500,8 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
                 T vr[NB], ur[NB];
 #pragma unroll
                 for (int q = 0; q < NB; q += Vec<T>::k) {
-                  lds16(Vs + r * NB + q, vr + q);
-                  lds16(Us + r * NB + q, ur + q);
+                  lds16(Vs + swz_index<T, NB>(r, q), vr + q);
+                  lds16(Us + swz_index<T, NB>(r, q), ur + q);
                 }
 #pragma unroll
                 for (int p = 0; p < NB; ++p)
@@ -510,8 +513,8 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
             myU[j] = u;
             myV[j] = v;
             if (tid < n) {
-              Us[tid * NB + j] = u;
-              Vs[tid * NB + j] = v;
+              Us[swz_index<T, NB>(tid, j)] = u;
+              Vs[swz_index<T, NB>(tid, j)] = v;
             }
             if (my_log == k + 2) misc[0] = tid;
             if (tid == 0) pivs[k >> 1] = lr != k + 1 ? -piv : piv;
@@ -556,12 +559,19 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
             ib1 = ib0 + 32;
             pb0 = ib0 < m ? alist[ib0] : 0;
             pb1 = ib1 < m ? alist[ib1] : 0;
+            // the columns' panel values, 16-byte loads of swizzled rows (conflict-free for
+            // consecutive active rows); rows past the end read row 0 and are zeroed
+#pragma unroll
+            for (int p = 0; p < NB; p += Vec<T>::k) {
+              lds16(Us + swz_index<T, NB>(pb0, p), ub0 + p);
+              lds16(Vs + swz_index<T, NB>(pb0, p), vb0 + p);
+              lds16(Us + swz_index<T, NB>(pb1, p), ub1 + p);
+              lds16(Vs + swz_index<T, NB>(pb1, p), vb1 + p);
+            }
 #pragma unroll
             for (int p = 0; p < NB; ++p) {
-              ub0[p] = ib0 < m ? Us[pb0 * NB + p] : T(0);
-              vb0[p] = ib0 < m ? Vs[pb0 * NB + p] : T(0);
-              ub1[p] = ib1 < m ? Us[pb1 * NB + p] : T(0);
-              vb1[p] = ib1 < m ? Vs[pb1 * NB + p] : T(0);
+              if (ib0 >= m) ub0[p] = vb0[p] = T(0);
+              if (ib1 >= m) ub1[p] = vb1[p] = T(0);
             }
           }
           T acc0[RT], acc1[RT], ua[RT][NB], va[RT][NB];
@@ -576,8 +586,8 @@ __global__ void __launch_bounds__(THREADS, THREADS > kNumThreads ? 1 : (sizeof(T
             off[rr] = tri_off(pa);
 #pragma unroll
             for (int p = 0; p < NB; p += Vec<T>::k) {
-              lds16(Us + pa * NB + p, ua[rr] + p);
-              lds16(Vs + pa * NB + p, va[rr] + p);
+              lds16(Us + swz_index<T, NB>(pa, p), ua[rr] + p);
+              lds16(Vs + swz_index<T, NB>(pa, p), va[rr] + p);
             }
           }
 #pragma unroll
