@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define NH_ABI_VERSION 7
+#define NH_ABI_VERSION 8
 
 enum {
   NH_OK = 0,
@@ -165,6 +165,9 @@ enum {
   NH_K_RESCONV_TC = 24,
   NH_K_REFINE = 25,
   NH_K_FUSED = 26,
+  NH_K_PF_ADJOINT = 27,
+  NH_K_PAIRING_VJP = 28,
+  NH_K_CNN_VJP = 29,
   NH_K_COUNT = 32
 };
 int nh_profile_enable(int on);
@@ -289,6 +292,41 @@ int nh_metropolis_steps_mixed(int8_t* spins, float* sign, double* logabs, int ba
                               const nh_backflow_params* p, int n_dirs, int first_exchange,
                               uint64_t seed, int64_t step0, int nsteps, int32_t* accepted,
                               void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Backward of the amplitude (the per-sample Jacobian that SR / AdamSR training consumes,
+ * code/train_pfaffian_16x16_tpm02.py:100-101).  FP32 throughout; n <= 224, 2 N <= 512,
+ * d in {8, 16, 32}. */
+
+/* Cotangent of the log-Pfaffian (the derivative of fermix.slogpf, code/backflow/models.py:210):
+ * G = d log|pf F| / dF = 1/2 F^{-T} for batch antisymmetric n x n FP32 matrices, from a
+ * Gauss-Jordan inverse with partial pivoting.  flags (batch,) or null: NH_FLAG_ZERO_PIVOT
+ * (singular) or NH_FLAG_NONFINITE; G is zero for such matrices. */
+int nh_pfaffian_adjoint(const float* F, int n, int batch, float* G, int32_t* flags, void* stream);
+
+/* The custom VJP of the occupied gather (code/backflow/pf_kernel.py:193-320, 354-365, per
+ * matrix): for the cotangent G (batch, n, n) of F = nh_pairing_occ(Y, idx, Wt),
+ * dY (batch, n, d) = sum_q (G - G^T)[p, q] Wt[blk(p, q), r(p, q), a] Y[q, a] and
+ * dWt (batch, 4, N, d) = sum over the pairs (p, q) of each block and displacement of
+ * G[p, q] Y[p, a] Y[q, a] (one table per matrix; a batched caller sums them). */
+int nh_pairing_occ_vjp(const float* Y, const int32_t* idx, const float* Wt, const float* G,
+                       int Lx, int Ly, int d, int n, int batch, float* dY, float* dWt,
+                       void* stream);
+
+/* Number of parameters P of the backflow CNN state: sum over layers of C_out C_in 9 + C_out,
+ * plus 3 N d (W) + 1 (theta).  0 for NH_NET_RESCONV. */
+int64_t nh_param_count(const nh_backflow_params* p);
+
+/* Per-sample Jacobian jac (batch, P) FP32 of log|psi_P(s)| (n_symm = 8) or log|psi(s)|
+ * (n_symm = 1) with respect to the parameters, in the order conv_w[0] (OIHW), conv_b[0], ...,
+ * conv_w[L-1], conv_b[L-1], W (3, N, d), theta; W and theta are the raw pairing parameters that
+ * p->Wt was built from (nh_build_wtilde).  The amplitude (sign, logabs, flags) is computed on the
+ * way with p's recompute policy; the backward runs on the FP32 CUDA-core path whatever p's
+ * cnn_mode / pf_mode.  Images are weighted by eta_g psi(g s) / sum_h eta_h psi(h s); a
+ * configuration whose projected amplitude is zero gets a zero row.  NH_NET_CNN only. */
+size_t nh_log_jacobian_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p);
+int nh_log_jacobian(const int8_t* spins, int batch, int n_symm, const nh_backflow_params* p,
+                    const float* W, float theta, float* jac, float* sign, double* logabs,
+                    int32_t* flags, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- Learned hop proposal ----
  * A periodic 3x3 CNN 2 -> 16 -> 16 -> 16 (tanh-GELU after layers 1 and 2) on the +-1 occupation

@@ -17,7 +17,8 @@ chains) and LearnedHop (Metropolis with the exact Hastings correction).
 """
 
 from ._lib import NativeLibraryError
-from .backflow import PairGeometry, PfaffianBackflow, build_wtilde, init_params, pairing_occ, slogpf
+from .backflow import (PairGeometry, PfaffianBackflow, build_wtilde, init_params, pairing_occ,
+                       pairing_occ_vjp, slogpf, slogpf_adjoint)
 from .operator import Hubbard
 from .proposal import HopProposal, LearnedHop, training_records
 from .sampler import MixSampler, ParticleHop, SiteExchange, random_spins
@@ -30,6 +31,8 @@ __all__ = [
     "build_wtilde",
     "init_params",
     "pairing_occ",
+    "pairing_occ_vjp",
+    "slogpf_adjoint",
     "slogpf",
     "Hubbard",
     "HopProposal",

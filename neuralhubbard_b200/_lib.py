@@ -17,7 +17,7 @@ NH_OK = 0
 NET_CNN, NET_RESCONV = 0, 1
 FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH, FLAG_REFINED, FLAG_CANCEL = 1, 2, 4, 8, 16
 FLAG_TIMEOUT = 32
-ABI_VERSION = 7
+ABI_VERSION = 8
 
 c_void_p, c_int, c_int64, c_uint64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64
 c_float, c_double, c_size_t = ctypes.c_float, ctypes.c_double, ctypes.c_size_t
@@ -112,6 +112,13 @@ SIGNATURES = {
                                      c_void_p, c_void_p, c_size_t, c_void_p]),
     "nh_proposal_adam_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int64,
                                       c_float, c_float, c_float, c_float, c_void_p, c_void_p]),
+    "nh_pfaffian_adjoint": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "nh_pairing_occ_vjp": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
+                                   c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "nh_param_count": (c_int64, [P_BF]),
+    "nh_log_jacobian_workspace_bytes": (c_size_t, [c_int, c_int, P_BF]),
+    "nh_log_jacobian": (c_int, [c_void_p, c_int, c_int, P_BF, c_void_p, c_float, c_void_p,
+                                c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "nh_metropolis_learned_workspace_bytes": (c_size_t, [c_int, c_int, P_BF]),
     "nh_metropolis_steps_learned": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, P_BF,
                                             P_Q, c_uint64, c_int64, c_int, c_void_p, c_void_p,
@@ -179,7 +186,7 @@ KERNEL_IDS = {
     "wtilde": 11, "pfaffian64": 12, "cnn64": 13, "flagged": 14, "pack": 15, "cnn_tc": 16,
     "pfaffian_tc": 17, "prop_sample": 18, "prop_forward": 19, "prop_backward": 20,
     "prop_adam": 21, "resconv": 22, "resconv64": 23, "resconv_tc": 24, "refine": 25,
-    "fused": 26,
+    "fused": 26, "pf_adjoint": 27, "pairing_vjp": 28, "cnn_vjp": 29,
 }
 K_COUNT = 32
 

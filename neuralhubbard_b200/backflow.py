@@ -6,6 +6,8 @@ Mirrors the reference's operator surface:
 * ``build_wtilde``        <- ``code/backflow/pf_kernel.py:107-124``
 * ``pairing_occ``         <- ``code/backflow/pf_kernel.py:335-351`` (forward only)
 * ``slogpf``              <- ``fermix.slogpf`` as called at ``code/backflow/models.py:210``
+* ``slogpf_adjoint``      <- the derivative of ``fermix.slogpf`` (d log|pf F| / dF)
+* ``pairing_occ_vjp``     <- the custom VJP of ``pairing_occ`` (``pf_kernel.py:193-320,354-365``)
 * ``PfaffianBackflow``    <- ``code/backflow/models.py:121-211`` with the backflow CNN of the
                              graded configurations (4 periodic 3x3 layers, 32 channels,
                              tanh-GELU between layers, 2-channel +-1 input).
@@ -115,6 +117,43 @@ def pairing_occ(Y: torch.Tensor, idx: torch.Tensor, Wt: torch.Tensor, geom: Pair
     _lib.call("nh_pairing_occ", Y.data_ptr(), idx.data_ptr(), Wt.data_ptr(), geom.LX, geom.LY, d,
               n, batch, F.data_ptr(), stream_ptr(Y.device))
     return F
+
+
+def pairing_occ_vjp(Y: torch.Tensor, idx: torch.Tensor, Wt: torch.Tensor, G: torch.Tensor,
+                    geom: PairGeometry):
+    """Cotangents (dY (..., n, d), dWt (..., 4, N, d)) of F = pairing_occ(Y, idx, Wt) for the
+    output cotangent G (..., n, n): ``_pairing_occ_bwd`` (``pf_kernel.py:354-365``) per matrix,
+    with dY formed from G - G^T and dWt from G; a batched caller sums dWt over the batch."""
+    Y = _require_cuda(Y, torch.float32, "Y")
+    idx = _require_cuda(idx, torch.int32, "idx")
+    Wt = _require_cuda(Wt, torch.float32, "Wt")
+    G = _require_cuda(G, torch.float32, "G")
+    n, d = Y.shape[-2], Y.shape[-1]
+    if (d != geom.d or idx.shape[-1] != n or tuple(Wt.shape) != (4, geom.N, d)
+            or tuple(G.shape[-2:]) != (n, n) or G.shape[:-2] != Y.shape[:-2]):
+        raise ValueError("pairing_occ_vjp: inconsistent shapes")
+    batch = int(np.prod(Y.shape[:-2])) if Y.dim() > 2 else 1
+    dY = torch.empty_like(Y)
+    dWt = torch.empty(Y.shape[:-2] + (4, geom.N, d), dtype=torch.float32, device=Y.device)
+    _lib.call("nh_pairing_occ_vjp", Y.data_ptr(), idx.data_ptr(), Wt.data_ptr(), G.data_ptr(),
+              geom.LX, geom.LY, d, n, batch, dY.data_ptr(), dWt.data_ptr(), stream_ptr(Y.device))
+    return dY, dWt
+
+
+def slogpf_adjoint(F: torch.Tensor):
+    """(G, flags): G = d log|pf F| / dF = 1/2 F^{-T} for antisymmetric F (..., n, n), FP32,
+    n even and at most 224; flags mark singular (FLAG_ZERO_PIVOT) or non-finite matrices, whose
+    G is zero."""
+    F = _require_cuda(F, torch.float32, "F")
+    n = F.shape[-1]
+    if F.shape[-2] != n:
+        raise ValueError("slogpf_adjoint: matrices must be square")
+    batch = int(np.prod(F.shape[:-2])) if F.dim() > 2 else 1
+    G = torch.empty_like(F)
+    flags = torch.empty(F.shape[:-2], dtype=torch.int32, device=F.device)
+    _lib.call("nh_pfaffian_adjoint", F.data_ptr(), n, batch, G.data_ptr(), flags.data_ptr(),
+              stream_ptr(F.device))
+    return G, flags
 
 
 # FP64 features (and an FP64 refinement of the log-Pfaffian against the FP64 pairing block) for
@@ -229,6 +268,12 @@ class PfaffianBackflow:
                                    self.Wt.data_ptr(), self.Wt64.data_ptr(), g.LX, g.LY, g.n_up,
                                    g.n_dn, self.channels, self.layers, self.cnn_mode, self.pf_mode,
                                    self.net, 0, self.cond_tau, self.cancel_tau, self.refine_tau)
+
+    @property
+    def param_count(self) -> int:
+        """Parameters of the backflow CNN state (the Jacobian's columns): conv weights and
+        biases per layer, W (3, N, d) and theta."""
+        return int(_lib.load().nh_param_count(ctypes.byref(self.c_params())))
 
     def features(self, spins: torch.Tensor) -> torch.Tensor:
         """(B, 2, N, d) backflow features of int8 configurations (B, 2N)."""

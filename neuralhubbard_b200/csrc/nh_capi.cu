@@ -836,4 +836,96 @@ int nh_metropolis_steps_learned(int8_t* spins, float* sign, double* logabs, int 
   return NH_OK;
 }
 
+// ------------------------------------------------------------------ backward (Jacobian)
+
+int nh_pfaffian_adjoint(const float* F, int n, int batch, float* G, int32_t* flags,
+                        void* stream) {
+  if (!F || !G || batch < 0) return fail(NH_ERR_INVALID, "pfaffian_adjoint: bad arguments");
+  if (n <= 0 || n % 2 || n > kGradMaxN)
+    return fail(NH_ERR_UNSUPPORTED, "pfaffian_adjoint: n = %d (even, <= %d)", n, kGradMaxN);
+  return launch_pf_adjoint(F, G, n, batch, nullptr, nullptr, 1, flags,
+                           static_cast<cudaStream_t>(stream));
+}
+
+int nh_pairing_occ_vjp(const float* Y, const int32_t* idx, const float* Wt, const float* G,
+                       int Lx, int Ly, int d, int n, int batch, float* dY, float* dWt,
+                       void* stream) {
+  if (!Y || !idx || !Wt || !G || !dY || !dWt || batch < 0 || n < 1)
+    return fail(NH_ERR_INVALID, "pairing_occ_vjp: bad arguments");
+  if (Lx < 1 || Ly < 1 || 2 * Lx * Ly > 512 || n > kGradMaxN)
+    return fail(NH_ERR_UNSUPPORTED, "pairing_occ_vjp: lattice %dx%d, n = %d", Lx, Ly, n);
+  return launch_pairing_vjp(G, Y, idx, Wt, Lx, Ly, d, n, 1, batch, dY, dWt, nullptr, 0, 0, 0.0f,
+                            static_cast<cudaStream_t>(stream));
+}
+
+int64_t nh_param_count(const nh_backflow_params* p) {
+  if (!p || p->net != NH_NET_CNN || p->layers < 1 || p->channels < 1) return 0;
+  const int64_t C = p->channels, N = (int64_t)p->Lx * p->Ly;
+  return (C * 2 * 9 + C) + (int64_t)(p->layers - 1) * (C * C * 9 + C) + 3 * N * (C / 2) + 1;
+}
+
+static const int kJacChunkItems = 4096;
+
+static int jac_chunk_samples(int batch, int n_symm) {
+  const int cs = kJacChunkItems / n_symm;
+  return batch < cs ? (batch > 0 ? batch : 1) : cs;
+}
+
+size_t nh_log_jacobian_workspace_bytes(int batch, int n_symm, const nh_backflow_params* p) {
+  if (!p || (n_symm != 1 && n_symm != 8)) return 0;
+  const size_t items = (size_t)jac_chunk_samples(batch, n_symm) * n_symm;
+  const size_t n = (size_t)(p->n_up + p->n_dn), d = (size_t)(p->channels / 2);
+  return pipeline_bytes((int)items, *p) + align256(items * n * n * sizeof(float)) +
+         align256(items * n * d * sizeof(float));
+}
+
+int nh_log_jacobian(const int8_t* spins, int batch, int n_symm, const nh_backflow_params* p,
+                    const float* W, float theta, float* jac, float* sign, double* logabs,
+                    int32_t* flags, void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_params(p);
+  if (rc) return rc;
+  if (!spins || !W || !jac || !sign || !logabs || batch < 0)
+    return fail(NH_ERR_INVALID, "log_jacobian: bad buffers");
+  if (n_symm != 1 && n_symm != 8)
+    return fail(NH_ERR_INVALID, "log_jacobian: n_symm %d (1 or 8)", n_symm);
+  const int n = p->n_up + p->n_dn, d = p->channels / 2, N = p->Lx * p->Ly;
+  if (p->net != NH_NET_CNN || !cnn_vjp_supported(*p) || n > kGradMaxN || 2 * N > 512 ||
+      (d != 8 && d != 16 && d != 32))
+    return fail(NH_ERR_UNSUPPORTED,
+                "log_jacobian: the backflow CNN with n <= %d, 2N <= 512, d in {8, 16, 32} "
+                "(got net %d, n %d, N %d, d %d)", kGradMaxN, p->net, n, N, d);
+  if (batch == 0) return NH_OK;
+  const size_t need = nh_log_jacobian_workspace_bytes(batch, n_symm, p);
+  if ((rc = check_workspace(workspace, workspace_bytes, need, "log_jacobian"))) return rc;
+  nh_backflow_params q = *p;  // the backward is FP32 on CUDA cores: so is its forward
+  q.cnn_mode = 0;
+  q.pf_mode = 0;
+  const int cs = jac_chunk_samples(batch, n_symm);
+  const int items = cs * n_symm;
+  PipelineBuffers b = carve_pipeline(workspace, items, q);
+  char* extra = static_cast<char*>(workspace) + pipeline_bytes(items, q);
+  float* Fbuf = reinterpret_cast<float*>(extra);
+  float* dYbuf = reinterpret_cast<float*>(extra + align256((size_t)items * n * n * sizeof(float)));
+  const int64_t P = nh_param_count(p);
+  const int64_t off_w = P - 1 - 3 * (int64_t)N * d;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  for (int c0 = 0; c0 < batch; c0 += cs) {
+    const int m = batch - c0 < cs ? batch - c0 : cs;
+    const int8_t* sp = spins + (size_t)c0 * 2 * N;
+    ConfigList cl{sp, nullptr, nullptr, nullptr, nullptr, m, n_symm};
+    if ((rc = run_pipeline(cl, q, b, sign + c0, logabs + c0, flags ? flags + c0 : nullptr, st)))
+      return rc;
+    if ((rc = launch_pairing(b.Y, b.idx, q.Wt, q.Lx, q.Ly, d, n, m * n_symm, Fbuf, st))) return rc;
+    if ((rc = launch_pf_adjoint(Fbuf, Fbuf, n, m * n_symm, b.pf_sign, b.pf_logabs, n_symm,
+                                nullptr, st)))
+      return rc;
+    float* jrow = jac + (size_t)c0 * P;
+    if ((rc = launch_pairing_vjp(Fbuf, b.Y, b.idx, q.Wt, q.Lx, q.Ly, d, n, n_symm, m, dYbuf,
+                                 nullptr, jrow, P, off_w, theta, st)))
+      return rc;
+    if ((rc = launch_cnn_vjp(sp, m, n_symm, q, dYbuf, b.idx, jrow, P, st))) return rc;
+  }
+  return NH_OK;
+}
+
 }  // extern "C"

@@ -20,6 +20,9 @@ constexpr int kPublicFlags = 0xFFFF;
 // memory, so n <= kRefineMaxN; beyond, flagged items are recomputed by the pivoted FP64 kernel.
 constexpr int kRefineMaxN = 224;
 constexpr size_t kRefineSmemLimit = 225 * 1024;
+// Backward of the amplitude (nh_grad.cu): the Gauss-Jordan inverse keeps the matrix in registers
+// and its transpose in shared memory, so n <= kGradMaxN.
+constexpr int kGradMaxN = 224;
 
 // ------------------------------------------------------------------ host-side error state
 void set_error(const char* fmt, ...);
@@ -464,6 +467,23 @@ int launch_mh_accept(int8_t* spins, float* sign, double* logabs, int batch, int 
                      const int32_t* c_count, const float* psign, const double* plogabs,
                      const float* lqr, uint64_t seed, int64_t step, int32_t* accepted,
                      cudaStream_t st);
+
+// Backward of the amplitude (nh_grad.cu).
+// G = scale 1/2 F^{-T} per matrix (in place allowed); with pf_sign set the scale is the image
+// weight of item i in its configuration (n_img images per configuration), else 1.
+int launch_pf_adjoint(const float* F, float* G, int n, int batch, const float* pf_sign,
+                      const double* pf_logabs, int n_img, int32_t* flags, cudaStream_t st);
+// Per item dY (may be null) and, with jac null, per item dWt (items, 4, N, d); with jac set the
+// images' dWt of each sample are summed and chained through build_wtilde's backward into
+// jac[sample * ld + off_w + (3 N d W values, theta)].
+int launch_pairing_vjp(const float* G, const float* Y, const int32_t* idx, const float* Wt,
+                       int Lx, int Ly, int d, int n, int n_img, int samples, float* dY,
+                       float* dWt, float* jac, int64_t ld, int64_t off_w, float theta,
+                       cudaStream_t st);
+// Convolution weight and bias cotangents of every sample's images, summed into jac[sample * ld].
+int launch_cnn_vjp(const int8_t* spins, int samples, int n_img, const nh_backflow_params& p,
+                   const float* dY, const int32_t* idx, float* jac, int64_t ld, cudaStream_t st);
+bool cnn_vjp_supported(const nh_backflow_params& p);
 
 int num_sms();
 

@@ -3,7 +3,9 @@
 
 The amplitude of a batch runs in one C-ABI call (``nh_amplitude``): symmetry images, backflow
 CNN, occupied pairing gather, log-Pfaffian and the signed log-sum over the 8 images of
-Flip(0) @ Flip(1) @ SpinInverse() (``code/states.py:274-279``).
+Flip(0) @ Flip(1) @ SpinInverse() (``code/states.py:274-279``).  ``Variational.jacobian`` gives
+the per-sample derivatives of log|psi| that SR / AdamSR consume
+(``code/train_pfaffian_16x16_tpm02.py:100-101``) in one call (``nh_log_jacobian``).
 """
 
 from __future__ import annotations
@@ -105,3 +107,34 @@ class Variational:
         if self.check_timeout:
             _lib.check_flags(flags, "nh_amplitude")
         return LogArray(sign, logabs, flags)
+
+    def jacobian(self, spins, max_parallel: Optional[int] = None):
+        """(LogArray, O): O (B, P) FP32 with O[b, k] = d log|psi_P(s_b)| / d theta_k (or of
+        log|psi(s_b)| without projection), columns in the order conv_w[0], conv_b[0], ...,
+        conv_w[L-1], conv_b[L-1], W (3, N, d), theta (``PfaffianBackflow.param_count``).
+        FP32 CUDA-core forward and backward; the backflow CNN with n <= 224."""
+        spins = as_spins(spins, self.device)
+        B = spins.shape[0]
+        if spins.dim() != 2 or spins.shape[1] != 2 * self.N:
+            raise ValueError(f"spins shape {tuple(spins.shape)} != (B, {2 * self.N})")
+        m = self.model
+        P = m.param_count
+        if P <= 0:
+            raise ValueError("jacobian: the backflow CNN state only")
+        sign = torch.empty(B, dtype=torch.float32, device=self.device)
+        logabs = torch.empty(B, dtype=torch.float64, device=self.device)
+        flags = torch.empty(B, dtype=torch.int32, device=self.device)
+        jac = torch.empty((B, P), dtype=torch.float32, device=self.device)
+        p = m.c_params()
+        lib = _lib.load()
+        chunk = min(B, max_parallel or self.max_parallel) if B else 1
+        nbytes = lib.nh_log_jacobian_workspace_bytes(chunk, self.n_symm, ctypes.byref(p))
+        ws = workspace(nbytes, self.device, "jacobian")
+        st = stream_ptr(self.device)
+        for c0 in range(0, B, chunk):
+            c1 = min(B, c0 + chunk)
+            _lib.call("nh_log_jacobian", spins[c0:c1].data_ptr(), c1 - c0, self.n_symm,
+                      ctypes.byref(p), m.W.data_ptr(), float(m.theta), jac[c0:].data_ptr(),
+                      sign[c0:].data_ptr(), logabs[c0:].data_ptr(), flags[c0:].data_ptr(),
+                      ws.data_ptr(), ws.numel(), st)
+        return LogArray(sign, logabs, flags), jac
