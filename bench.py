@@ -967,6 +967,8 @@ def run_reference(args) -> None:
 #   amplitude          16x16 projected amplitudes, 1024 x 8 images, tcgen05 CNN + staged FP32
 #                      Pfaffian + default refinement (the benchmark's chosen form)
 #   amplitude_plain    the same on the plain form (fused FP32 CNN + Pfaffian kernel)
+#   jacobian           16x16 per-sample Jacobian of log|psi_P|, 128 x 8 images (Pfaffian adjoint,
+#                      pairing VJP and CNN VJP kernels after the amplitude pipeline)
 
 def _model(L, cnn_mode=0):
     import neuralhubbard_b200 as nh
@@ -1122,11 +1124,23 @@ def case_amplitude_plain(repeat):
     _amplitude(repeat, 0)
 
 
+def case_jacobian(repeat):
+    import torch
+
+    import neuralhubbard_b200 as nh
+
+    model, ne = _model(16)
+    state = nh.Variational(model, symm=True)
+    s = torch.from_numpy(nh.random_spins(np.random.default_rng(10), 128, 256, ne, ne)).cuda()
+    for _ in range(repeat):
+        state.jacobian(s)
+
+
 CASES = {"pairing": case_pairing, "hops": case_hops, "eloc": case_eloc,
          "proposal_sample": case_proposal_sample, "proposal_backward": case_proposal_backward,
          "resconv_tc": case_resconv_tc, "resconv": case_resconv,
          "refine": case_refine, "amplitude": case_amplitude,
-         "amplitude_plain": case_amplitude_plain}
+         "amplitude_plain": case_amplitude_plain, "jacobian": case_jacobian}
 
 
 

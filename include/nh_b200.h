@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define NH_ABI_VERSION 8
+#define NH_ABI_VERSION 9
 
 enum {
   NH_OK = 0,
@@ -57,6 +57,10 @@ enum {
 /* Backflow networks (nh_backflow_params.net). */
 #define NH_NET_CNN 0     /* periodic 3x3 CNN on the +-1 occupation image (layers conv layers) */
 #define NH_NET_RESCONV 1 /* residual CNN of the released states (layers residual blocks) */
+
+/* Ansatz (nh_backflow_params.ansatz). */
+#define NH_ANSATZ_PFAFFIAN 0 /* psi = pf(F[idx, idx]) (code/backflow/models.py:121-211) */
+#define NH_ANSATZ_BCS 1      /* psi = det(F_ud) (code/backflow/models.py:214-302) */
 
 /* Parameters of the backflow network (device pointers).
  * net:           NH_NET_CNN or NH_NET_RESCONV.
@@ -101,7 +105,16 @@ enum {
  *                sum_g |psi(g s)| > cancel_tau |sum_g eta_g psi(g s)|, amplifies the FP32
  *                error of its images by that factor; with cancel_tau > 0 (and Wt64 set) all its
  *                images are recomputed in FP64 and the output carries NH_FLAG_CANCEL.  <= 0:
- *                off (the flag is then never set). */
+ *                off (the flag is then never set).
+ * ansatz:        NH_ANSATZ_PFAFFIAN, or NH_ANSATZ_BCS: psi(s) = det F (-1)^(n_up (n_up - 1) / 2)
+ *                x fermion_inverse_sign(s) with the occupied up x down block
+ *                F[p, q] = sum_a y_up[p, a] Wt[1, site_p - site_q, a] y_dn[q, a]
+ *                + delta_d fd(site_p - site_q), fd = -1 on x bonds and +1 on y bonds
+ *                (code/backflow/models.py:214-302, bcs_kernel.py:1-70).  Wt is the table of
+ *                nh_build_wtilde for W = [W_ud, 0, 0] (block 1 is read).  Needs n_up == n_dn
+ *                <= 224, d = 16 and pf_mode 0; the FP64 recompute of flagged images (cond_tau,
+ *                cancel_tau) covers n_up <= 128.
+ * delta_d:       the BCS d-wave amplitude (ignored by the Pfaffian ansatz). */
 typedef struct {
   const float* conv_w;
   const float* conv_b;
@@ -116,10 +129,11 @@ typedef struct {
   int32_t cnn_mode;
   int32_t pf_mode;
   int32_t net;
-  int32_t reserved;
+  int32_t ansatz;
   double cond_tau;
   double cancel_tau;
   double refine_tau;
+  double delta_d;
 } nh_backflow_params;
 
 /* Hubbard model H = -sum t_ij c+_i c_j + U sum n_up n_dn; n_dirs = 4 (nearest) or 8
@@ -168,6 +182,8 @@ enum {
   NH_K_PF_ADJOINT = 27,
   NH_K_PAIRING_VJP = 28,
   NH_K_CNN_VJP = 29,
+  NH_K_DET = 30,
+  NH_K_DET64 = 31,
   NH_K_COUNT = 32
 };
 int nh_profile_enable(int on);

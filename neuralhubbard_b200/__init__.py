@@ -17,8 +17,8 @@ chains) and LearnedHop (Metropolis with the exact Hastings correction).
 """
 
 from ._lib import NativeLibraryError
-from .backflow import (PairGeometry, PfaffianBackflow, build_wtilde, init_params, pairing_occ,
-                       pairing_occ_vjp, slogpf, slogpf_adjoint)
+from .backflow import (BCSBackflow, PairGeometry, PfaffianBackflow, build_wtilde, init_params,
+                       pairing_occ, pairing_occ_vjp, slogpf, slogpf_adjoint)
 from .operator import Hubbard
 from .proposal import HopProposal, LearnedHop, training_records
 from .sampler import MixSampler, ParticleHop, SiteExchange, random_spins
@@ -28,6 +28,7 @@ __all__ = [
     "NativeLibraryError",
     "PairGeometry",
     "PfaffianBackflow",
+    "BCSBackflow",
     "build_wtilde",
     "init_params",
     "pairing_occ",

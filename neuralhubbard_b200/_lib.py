@@ -15,9 +15,10 @@ LIB_PATH = os.path.join(_HERE, "libnh_b200.so")
 
 NH_OK = 0
 NET_CNN, NET_RESCONV = 0, 1
+ANSATZ_PFAFFIAN, ANSATZ_BCS = 0, 1
 FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH, FLAG_REFINED, FLAG_CANCEL = 1, 2, 4, 8, 16
 FLAG_TIMEOUT = 32
-ABI_VERSION = 8
+ABI_VERSION = 9
 
 c_void_p, c_int, c_int64, c_uint64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64
 c_float, c_double, c_size_t = ctypes.c_float, ctypes.c_double, ctypes.c_size_t
@@ -44,10 +45,11 @@ class BackflowParams(ctypes.Structure):
         ("cnn_mode", ctypes.c_int32),
         ("pf_mode", ctypes.c_int32),
         ("net", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("ansatz", ctypes.c_int32),
         ("cond_tau", c_double),
         ("cancel_tau", c_double),
         ("refine_tau", c_double),
+        ("delta_d", c_double),
     ]
 
 
@@ -186,7 +188,7 @@ KERNEL_IDS = {
     "wtilde": 11, "pfaffian64": 12, "cnn64": 13, "flagged": 14, "pack": 15, "cnn_tc": 16,
     "pfaffian_tc": 17, "prop_sample": 18, "prop_forward": 19, "prop_backward": 20,
     "prop_adam": 21, "resconv": 22, "resconv64": 23, "resconv_tc": 24, "refine": 25,
-    "fused": 26, "pf_adjoint": 27, "pairing_vjp": 28, "cnn_vjp": 29,
+    "fused": 26, "pf_adjoint": 27, "pairing_vjp": 28, "cnn_vjp": 29, "det": 30, "det64": 31,
 }
 K_COUNT = 32
 

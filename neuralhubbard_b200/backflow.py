@@ -261,13 +261,17 @@ class PfaffianBackflow:
         self.Wt, self.Wt64 = build_wtilde(self.W, self.theta, self.geom, fp64=True)
         self.host_params = params
 
+    ansatz = _lib.ANSATZ_PFAFFIAN
+    delta_d = 0.0
+
     def c_params(self) -> _lib.BackflowParams:
         g = self.geom
         return _lib.BackflowParams(self.conv_w.data_ptr(), self.conv_b.data_ptr(),
                                    self.conv_w_packed.data_ptr(), _ptr(self.conv_w_tc),
                                    self.Wt.data_ptr(), self.Wt64.data_ptr(), g.LX, g.LY, g.n_up,
                                    g.n_dn, self.channels, self.layers, self.cnn_mode, self.pf_mode,
-                                   self.net, 0, self.cond_tau, self.cancel_tau, self.refine_tau)
+                                   self.net, self.ansatz, self.cond_tau, self.cancel_tau,
+                                   self.refine_tau, float(self.delta_d))
 
     @property
     def param_count(self) -> int:
@@ -285,3 +289,33 @@ class PfaffianBackflow:
         _lib.call("nh_cnn_forward", spins.data_ptr(), B, ctypes.byref(p), out.data_ptr(),
                   stream_ptr(spins.device))
         return out
+
+
+class BCSBackflow(PfaffianBackflow):
+    """The BCS-backflow state of ``code/backflow/models.py:214-302``:
+    psi(s) = det F (-1)^(n_up (n_up - 1) / 2) fermion_inverse_sign(s) with the occupied up x down
+    block F[p, q] = sum_a y_up[p, a] Wt_ud[site_p - site_q, a] y_dn[q, a] + delta_d fd(p, q)
+    (``bcs_kernel.py:1-70``; fd the nearest-neighbour d-wave form factor).  The features are the
+    two spin halves of the backflow network's output (d = 16: 32 channels); parameters are those
+    of ``PfaffianBackflow`` with W of shape (N, d) and ``delta_d`` (default 0.1, as
+    ``models.py:246``).  n_up == n_dn <= 224; FP64 recompute of flagged images up to 128."""
+
+    ansatz = _lib.ANSATZ_BCS
+
+    def __init__(self, Lx: int, Ly: int, n_up: int, n_dn: int, params: Optional[dict] = None,
+                 seed: int = 0, **kw):
+        if params is None:
+            params = init_params(Lx, Ly, kw.get("channels", 32), kw.get("layers", 4), seed=seed)
+            params["W"] = params["W"][0]
+            params["delta_d"] = 0.1
+        super().__init__(Lx, Ly, n_up, n_dn, params=params, seed=seed, **kw)
+
+    def set_params(self, params: dict) -> None:
+        W = np.asarray(params["W"], np.float32)
+        if W.ndim != 2:
+            raise ValueError(f"BCS W must be (N, d), got {W.shape}")
+        self.delta_d = float(params.get("delta_d", 0.1))
+        full = dict(params)
+        full["W"] = np.stack([W, np.zeros_like(W), np.zeros_like(W)])
+        super().set_params(full)
+        self.host_params = params

@@ -178,6 +178,31 @@ int run_pipeline(const ConfigList& cl, const nh_backflow_params& p, const Pipeli
     rc = launch_cnn(c, st);
   }
   if (rc) return rc;
+  if (p.ansatz == NH_ANSATZ_BCS) {
+    // Determinant of the up x down block, FP32; flagged images again from FP64 features.
+    DetLaunch dq{b.Y, b.idx, p.Wt, p.Lx, p.Ly, p.n_up, d, p.delta_d, cl.n_cfg_dev, cl.G,
+                 max_items, nullptr, b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags,
+                 b.pf_ratio, p.cond_tau, 0, false};
+    if ((rc = launch_det(dq, st))) return rc;
+    const bool fp64 = p.Wt64 && det_supported(p.n_up, d, true) &&
+                      (p.cond_tau > 0.0 || (p.cancel_tau > 0.0 && cl.G > 1));
+    if (fp64) {
+      if ((rc = launch_image_mark(b.pf_sign, b.pf_logabs, b.pf_flags, b.pf_ratio, cl.G, cl.n_cfg,
+                                  cl.n_cfg_dev, p.cancel_tau, p.cond_tau, p.cond_tau > 1.0, st)))
+        return rc;
+      if ((rc = launch_flagged(b.pf_flags, max_items, cl.n_cfg_dev, cl.G, b.list, b.count, st)))
+        return rc;
+      CnnLaunch c64{&cl, &p, 1, true, b.list, b.count, max_items, nullptr, b.Y64, b.idx64,
+                    b.item_sign, b.cnn_act};
+      if ((rc = launch_cnn(c64, st))) return rc;
+      DetLaunch d64{b.Y64, b.idx64, p.Wt64, p.Lx, p.Ly, p.n_up, d, p.delta_d, b.count, 1,
+                    max_items, b.list, b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, nullptr,
+                    0.0, NH_FLAG_GROWTH | NH_FLAG_REFINED, true};
+      if ((rc = launch_det(d64, st))) return rc;
+    }
+    return launch_combine(b.pf_sign, b.pf_logabs, b.pf_flags, cl.G, cl.n_cfg, cl.n_cfg_dev, sign,
+                          logabs, flags, p.cancel_tau, tc ? b.err : nullptr, st);
+  }
   const bool refine = b.perm != nullptr;  // n <= kRefineMaxN
   PfGatherArgs g{b.Y, b.idx, p.Wt, p.Lx, p.Ly, d, n, cl.n_cfg_dev, cl.G, max_items, nullptr,
                  b.item_sign, b.pf_sign, b.pf_logabs, b.pf_flags, p.cond_tau, 0, false, b.pf_tri};
@@ -247,7 +272,7 @@ struct FusedBuffers {
 };
 
 static bool fused_ok(const nh_backflow_params& p) {
-  return fused_supported(p) && p.n_up + p.n_dn <= kRefineMaxN;
+  return p.ansatz == NH_ANSATZ_PFAFFIAN && fused_supported(p) && p.n_up + p.n_dn <= kRefineMaxN;
 }
 
 static size_t fused_bytes(size_t items, const nh_backflow_params& p) {
@@ -372,6 +397,12 @@ static int check_params(const nh_backflow_params* p) {
   if (p->pf_mode < 0 || p->pf_mode > 1) return fail(NH_ERR_INVALID, "pf_mode %d", p->pf_mode);
   if (p->pf_mode == 1 && n > kNumThreads)
     return fail(NH_ERR_UNSUPPORTED, "pf_mode 1 needs n <= %d", kNumThreads);
+  if (p->ansatz != NH_ANSATZ_PFAFFIAN && p->ansatz != NH_ANSATZ_BCS)
+    return fail(NH_ERR_INVALID, "ansatz %d (NH_ANSATZ_PFAFFIAN or NH_ANSATZ_BCS)", p->ansatz);
+  if (p->ansatz == NH_ANSATZ_BCS &&
+      (p->n_up != p->n_dn || !det_supported(p->n_up, d, false) || p->pf_mode != 0))
+    return fail(NH_ERR_UNSUPPORTED, "BCS ansatz: n_up == n_dn <= %d, d = 16, pf_mode 0 "
+                "(got %d, %d, d %d, pf_mode %d)", kDetMaxNh, p->n_up, p->n_dn, d, p->pf_mode);
   return NH_OK;
 }
 
@@ -889,7 +920,8 @@ int nh_log_jacobian(const int8_t* spins, int batch, int n_symm, const nh_backflo
   if (n_symm != 1 && n_symm != 8)
     return fail(NH_ERR_INVALID, "log_jacobian: n_symm %d (1 or 8)", n_symm);
   const int n = p->n_up + p->n_dn, d = p->channels / 2, N = p->Lx * p->Ly;
-  if (p->net != NH_NET_CNN || !cnn_vjp_supported(*p) || n > kGradMaxN || 2 * N > 512 ||
+  if (p->net != NH_NET_CNN || p->ansatz != NH_ANSATZ_PFAFFIAN || !cnn_vjp_supported(*p) ||
+      n > kGradMaxN || 2 * N > 512 ||
       (d != 8 && d != 16 && d != 32))
     return fail(NH_ERR_UNSUPPORTED,
                 "log_jacobian: the backflow CNN with n <= %d, 2N <= 512, d in {8, 16, 32} "

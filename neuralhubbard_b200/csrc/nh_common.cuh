@@ -23,6 +23,10 @@ constexpr size_t kRefineSmemLimit = 225 * 1024;
 // Backward of the amplitude (nh_grad.cu): the Gauss-Jordan inverse keeps the matrix in registers
 // and its transpose in shared memory, so n <= kGradMaxN.
 constexpr int kGradMaxN = 224;
+// BCS determinant (nh_det.cu): the up x down block lives in registers (FP32 up to 224 rows, FP64
+// up to 128).
+constexpr int kDetMaxNh = 224;
+constexpr int kDetMaxNh64 = 128;
 
 // ------------------------------------------------------------------ host-side error state
 void set_error(const char* fmt, ...);
@@ -484,6 +488,29 @@ int launch_pairing_vjp(const float* G, const float* Y, const int32_t* idx, const
 int launch_cnn_vjp(const int8_t* spins, int samples, int n_img, const nh_backflow_params& p,
                    const float* dY, const int32_t* idx, float* jac, int64_t ld, cudaStream_t st);
 bool cnn_vjp_supported(const nh_backflow_params& p);
+
+// BCS determinant of every item (or of the items of a device list) from its occupied rows.
+struct DetLaunch {
+  const void* Y;       // (slots, n, d) float or double
+  const int32_t* idx;  // (slots, n)
+  const void* Wt;      // (4, N, d) float or double
+  int Lx, Ly, nh, d;
+  double delta_d;
+  const int32_t* count_dev;  // device work count (times count_mult) or null
+  int count_mult;
+  int n_slots;               // host upper bound of the slots
+  const int32_t* slot_item;  // slot -> item, null: identity
+  const float* item_sign;
+  float* sign;
+  double* logabs;
+  int32_t* flags;
+  float* ratio;
+  double cond_tau;
+  int flag_or;
+  bool fp64;
+};
+bool det_supported(int nh, int d, bool fp64);
+int launch_det(const DetLaunch& q, cudaStream_t st);
 
 int num_sms();
 

@@ -200,7 +200,7 @@ def test_residual_network_argument_checks():
     def amplitude(**kw):
         f = dict(conv_w=4096, conv_b=4096, conv_w_packed=4096, conv_w_tc=4096, Wt=4096,
                  Wt64=4096, Lx=16, Ly=16, n_up=112, n_dn=112, channels=64, layers=16,
-                 cnn_mode=0, pf_mode=0, net=_lib.NET_RESCONV, reserved=0, cond_tau=100.0,
+                 cnn_mode=0, pf_mode=0, net=_lib.NET_RESCONV, ansatz=0, cond_tau=100.0,
                  cancel_tau=8.0)
         f.update(kw)
         prm = _lib.BackflowParams(**f)
@@ -210,6 +210,12 @@ def test_residual_network_argument_checks():
     assert amplitude(cnn_mode=1) == -2
     assert amplitude(cnn_mode=2, Lx=8, Ly=8, n_up=28, n_dn=28) == -2
     assert amplitude(net=7) == -1 and b"net 7" in lib.nh_last_error()
+    assert amplitude(ansatz=5) == -1 and b"ansatz 5" in lib.nh_last_error()
+    # BCS ansatz: equal spin numbers, d = 16, no tensor-memory Pfaffian
+    assert amplitude(net=_lib.NET_CNN, channels=32, layers=4, ansatz=_lib.ANSATZ_BCS,
+                     n_dn=110) == -2 and b"BCS" in lib.nh_last_error()
+    assert amplitude(net=_lib.NET_CNN, channels=32, layers=4, ansatz=_lib.ANSATZ_BCS,
+                     pf_mode=1) == -2
 
 
 def test_timeout_flag_raises():
