@@ -184,7 +184,8 @@ enum {
   NH_K_CNN_VJP = 29,
   NH_K_DET = 30,
   NH_K_DET64 = 31,
-  NH_K_COUNT = 32
+  NH_K_OBS = 32,
+  NH_K_COUNT = 40
 };
 int nh_profile_enable(int on);
 int nh_profile_read(double* ms, int64_t* launches, int n_ids);
@@ -343,6 +344,29 @@ size_t nh_log_jacobian_workspace_bytes(int batch, int n_symm, const nh_backflow_
 int nh_log_jacobian(const int8_t* spins, int batch, int n_symm, const nh_backflow_params* p,
                     const float* W, float theta, float* jac, float* sign, double* logabs,
                     int32_t* flags, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- Packed observables (code/measure/transverse_spin.py:44-119, dwave_packed.py:24-103):
+ * one operator family O = sum_t O_t per call.  Every sample's connections s -> s' of the terms
+ * go through the amplitude pipeline (as for the local energy; the call synchronises the stream
+ * once to read the number of connections), and the local values
+ * <s|O_t|s'> psi(s') / psi(s) are summed per term t over the batch in a fixed order and divided
+ * by batch; the diagonal term of the family comes from the occupations.  out (device, FP64):
+ *   NH_OBS_TRANSVERSE_SPIN  arg0 = reference site a: out (2, N), [0, r] = <S+_a S-_{a+r}>,
+ *                           [1, r] = <S-_a S+_{a+r}> (r = x Ly + y, periodic), r = 0 holding
+ *                           n_up (1 - n_dn) and n_dn (1 - n_up) at a;
+ *   NH_OBS_PAIR             arg0, arg1 = sites a, b of A+ = c+_{a up} c+_{b dn}: out (4 N),
+ *                           [t] = <A+(a, b) A(c_t, d_t)> over the bonds t = 4 site + 2 axis + o
+ *                           (axis 0: +x, 1: +y; (c, d) = (site, site + axis) for o = 0 and
+ *                           swapped for o = 1); the term (c, d) = (a, b) is n_{a up} n_{b dn};
+ *   NH_OBS_HOP              arg0 = site i, arg1 = spin (0 up, 1 down): out (N),
+ *                           [j] = <c+_{i s} c_{j s}>, [i] = n_{i s}. */
+#define NH_OBS_TRANSVERSE_SPIN 0
+#define NH_OBS_PAIR 1
+#define NH_OBS_HOP 2
+size_t nh_observable_workspace_bytes(int batch, int n_symm, int kind, const nh_backflow_params* p);
+int nh_observable(const int8_t* spins, const float* sign, const double* logabs, int batch,
+                  int n_symm, const nh_backflow_params* p, int kind, int arg0, int arg1,
+                  double* out, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- Learned hop proposal ----
  * A periodic 3x3 CNN 2 -> 16 -> 16 -> 16 (tanh-GELU after layers 1 and 2) on the +-1 occupation

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libnh_b200.so")
 NH_OK = 0
 NET_CNN, NET_RESCONV = 0, 1
 ANSATZ_PFAFFIAN, ANSATZ_BCS = 0, 1
+OBS_TRANSVERSE_SPIN, OBS_PAIR, OBS_HOP = 0, 1, 2
 FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH, FLAG_REFINED, FLAG_CANCEL = 1, 2, 4, 8, 16
 FLAG_TIMEOUT = 32
 ABI_VERSION = 9
@@ -121,6 +122,9 @@ SIGNATURES = {
     "nh_log_jacobian_workspace_bytes": (c_size_t, [c_int, c_int, P_BF]),
     "nh_log_jacobian": (c_int, [c_void_p, c_int, c_int, P_BF, c_void_p, c_float, c_void_p,
                                 c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "nh_observable_workspace_bytes": (c_size_t, [c_int, c_int, c_int, P_BF]),
+    "nh_observable": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, P_BF, c_int, c_int,
+                              c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
     "nh_metropolis_learned_workspace_bytes": (c_size_t, [c_int, c_int, P_BF]),
     "nh_metropolis_steps_learned": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, P_BF,
                                             P_Q, c_uint64, c_int64, c_int, c_void_p, c_void_p,
@@ -189,8 +193,9 @@ KERNEL_IDS = {
     "pfaffian_tc": 17, "prop_sample": 18, "prop_forward": 19, "prop_backward": 20,
     "prop_adam": 21, "resconv": 22, "resconv64": 23, "resconv_tc": 24, "refine": 25,
     "fused": 26, "pf_adjoint": 27, "pairing_vjp": 28, "cnn_vjp": 29, "det": 30, "det64": 31,
+    "observable": 32,
 }
-K_COUNT = 32
+K_COUNT = 40
 
 
 def profile_enable(on: bool) -> None:

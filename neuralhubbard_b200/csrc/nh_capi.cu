@@ -960,4 +960,115 @@ int nh_log_jacobian(const int8_t* spins, int batch, int n_symm, const nh_backflo
   return NH_OK;
 }
 
+// ------------------------------------------------------------------ packed observables
+
+struct ObsLayout {
+  int32_t *counts, *owner, *from, *to, *bin, *chunk_cnt;
+  int64_t* offsets;
+  double *hval, *clogabs, *V;
+  float* csign;
+  int n_chunks;
+  void* pipe;
+  size_t bytes;
+};
+
+static ObsLayout obs_layout(void* ws, int batch, int n_symm, int kind, int chunk,
+                            const nh_backflow_params* p) {
+  const size_t T = (size_t)obs_terms(kind, p->Lx * p->Ly);
+  const size_t cmax = (size_t)batch * T;
+  char* q = static_cast<char*>(ws);
+  ObsLayout L;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char* r = q ? q + off : nullptr;
+    off += align256(bytes);
+    return r;
+  };
+  L.counts = reinterpret_cast<int32_t*>(take((size_t)batch * 4));
+  L.offsets = reinterpret_cast<int64_t*>(take((size_t)(batch + 1) * 8));
+  L.owner = reinterpret_cast<int32_t*>(take(cmax * 4));
+  L.from = reinterpret_cast<int32_t*>(take(cmax * 4));
+  L.to = reinterpret_cast<int32_t*>(take(cmax * 4));
+  L.bin = reinterpret_cast<int32_t*>(take(cmax * 4));
+  L.hval = reinterpret_cast<double*>(take(cmax * 8));
+  L.csign = reinterpret_cast<float*>(take(cmax * 4));
+  L.clogabs = reinterpret_cast<double*>(take(cmax * 8));
+  L.V = reinterpret_cast<double*>(take((size_t)batch * T * 8));
+  const size_t ch = chunk > 0 ? (size_t)chunk : (cmax > 0 ? cmax : 1);
+  L.n_chunks = (int)((cmax + ch - 1) / ch);
+  L.chunk_cnt = reinterpret_cast<int32_t*>(take((size_t)(L.n_chunks > 0 ? L.n_chunks : 1) * 4));
+  L.pipe = take(chunk > 0 ? pipeline_bytes(chunk * n_symm, *p) : fused_bytes(cmax * n_symm, *p));
+  L.bytes = off;
+  return L;
+}
+
+size_t nh_observable_workspace_bytes(int batch, int n_symm, int kind, const nh_backflow_params* p) {
+  if (!p || batch <= 0 || kind < NH_OBS_TRANSVERSE_SPIN || kind > NH_OBS_HOP) return 0;
+  return obs_layout(nullptr, batch, n_symm, kind, eloc_chunk(0, p), p).bytes;
+}
+
+int nh_observable(const int8_t* spins, const float* sign, const double* logabs, int batch,
+                  int n_symm, const nh_backflow_params* p, int kind, int arg0, int arg1,
+                  double* out, void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_params(p);
+  if (rc) return rc;
+  if (!spins || !sign || !logabs || !out || batch < 0)
+    return fail(NH_ERR_INVALID, "observable: bad buffers");
+  if (n_symm != 1 && n_symm != 8) return fail(NH_ERR_INVALID, "observable: n_symm %d", n_symm);
+  const int Lx = p->Lx, Ly = p->Ly, N = Lx * Ly;
+  if (kind < NH_OBS_TRANSVERSE_SPIN || kind > NH_OBS_HOP)
+    return fail(NH_ERR_INVALID, "observable: kind %d", kind);
+  if (2 * N > 32 * 64) return fail(NH_ERR_UNSUPPORTED, "observable: N = %d (<= 1024)", N);
+  if (arg0 < 0 || arg0 >= N || (kind == NH_OBS_PAIR && (arg1 < 0 || arg1 >= N)) ||
+      (kind == NH_OBS_HOP && arg1 != 0 && arg1 != 1))
+    return fail(NH_ERR_INVALID, "observable: arguments %d, %d", arg0, arg1);
+  if (batch == 0) return NH_OK;
+  const int chunk = eloc_chunk(0, p);
+  const size_t need = nh_observable_workspace_bytes(batch, n_symm, kind, p);
+  if ((rc = check_workspace(workspace, workspace_bytes, need, "observable"))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  ObsLayout L = obs_layout(workspace, batch, n_symm, kind, chunk, p);
+  // Diagonal term's bin: r = 0 (and N), (c, d) = (a, b) when that pair is a bond, j = i.
+  int diag_bin = kind == NH_OBS_HOP ? arg0 : (kind == NH_OBS_TRANSVERSE_SPIN ? 0 : -1);
+  if (kind == NH_OBS_PAIR) {
+    for (int t = 0; t < 4 * N && diag_bin < 0; ++t) {
+      const int site = t >> 2, axis = (t >> 1) & 1, o = t & 1, x = site / Ly, y = site % Ly;
+      const int hi = axis == 0 ? ((x + 1) % Lx) * Ly + y : x * Ly + (y + 1) % Ly;
+      if ((o == 0 ? site : hi) == arg0 && (o == 0 ? hi : site) == arg1) diag_bin = t;
+    }
+  }
+  if ((rc = launch_obs_list(spins, batch, Lx, Ly, kind, arg0, arg1, L.counts, L.offsets, L.owner,
+                            L.from, L.to, L.hval, L.bin, st)))
+    return rc;
+  int64_t total = 0;
+  if ((rc = check_cuda(cudaMemcpyAsync(&total, L.offsets + batch, sizeof(int64_t),
+                                       cudaMemcpyDeviceToHost, st),
+                       "observable: read connection count")))
+    return rc;
+  if ((rc = check_cuda(cudaStreamSynchronize(st), "observable: sync"))) return rc;
+  if (total > 0) {
+    const int64_t cmax = (int64_t)batch * obs_terms(kind, N);
+    if ((rc = launch_chunk_counts(L.offsets + batch, L.n_chunks, chunk > 0 ? chunk : (int)cmax,
+                                  L.chunk_cnt, st)))
+      return rc;
+    if (chunk == 0) {
+      ConfigList cl{spins, L.owner, L.from, L.to, L.chunk_cnt, (int)cmax, n_symm};
+      FusedBuffers fb = carve_fused(L.pipe, (size_t)cmax * n_symm, *p);
+      if ((rc = run_pipeline_fused(cl, *p, fb, L.csign, L.clogabs, nullptr, st))) return rc;
+    } else {
+      PipelineBuffers b = carve_pipeline(L.pipe, chunk * n_symm, *p);
+      const int used = (int)((total + chunk - 1) / chunk);
+      for (int i = 0; i < used; ++i) {
+        const int64_t c0 = (int64_t)i * chunk;
+        ConfigList cl{spins, L.owner + c0, L.from + c0, L.to + c0, L.chunk_cnt + i, chunk,
+                      n_symm};
+        if ((rc = run_pipeline(cl, *p, b, L.csign + c0, L.clogabs + c0, nullptr, st))) return rc;
+      }
+    }
+  }
+  return launch_obs_reduce(spins, sign, logabs, batch, N, kind, arg0, arg1, diag_bin,
+                           L.offsets + batch, L.owner, L.bin, L.hval, L.csign, L.clogabs, L.V, out,
+                           st);
+}
+
 }  // extern "C"

@@ -512,6 +512,18 @@ struct DetLaunch {
 bool det_supported(int nh, int d, bool fp64);
 int launch_det(const DetLaunch& q, cudaStream_t st);
 
+// Packed observables (nh_obs.cu): terms per sample of a family, the connection list (counts,
+// scan, emit in term order), and the binned reduction of the local values.
+int obs_terms(int kind, int N);
+int launch_obs_list(const int8_t* spins, int batch, int Lx, int Ly, int kind, int a0, int a1,
+                    int32_t* counts, int64_t* offsets, int32_t* owner, int32_t* from,
+                    int32_t* to, double* hval, int32_t* bin, cudaStream_t st);
+int launch_obs_reduce(const int8_t* spins, const float* sign, const double* logabs, int batch,
+                      int N, int kind, int a0, int a1, int diag_bin, const int64_t* total,
+                      const int32_t* owner, const int32_t* bin, const double* hval,
+                      const float* csign, const double* clogabs, double* V, double* out,
+                      cudaStream_t st);
+
 int num_sms();
 
 // Per-kernel CUDA-event timing (enabled by nh_profile_enable).  Construct before the launch,
