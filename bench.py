@@ -22,6 +22,8 @@ ragged local energy at 8x8, 16x16 and 24x24, one CUDA-graph replay each; ``large
 against the library's all-FP64 path, and near-nodal log-Pfaffians at the slogpf boundary.
 ``resconv`` (1 GPU) times the released states' residual network (16 blocks x 64 channels) on
 CUDA cores and on the tensor cores, with E/N of the released 16x16 state on 512 of its chains.
+``extensions`` (1 GPU) times the per-sample Jacobian of log|psi_P|, the BCS-backflow ansatz (with
+its error against the BCS all-FP64 form) and the packed observables.
 
 Under torchrun each rank evaluates its own 8192 configurations (weak scaling); the time is the
 maximum over ranks of the summed per-step CUDA-event durations.  ``--impl reference`` times the
@@ -556,6 +558,86 @@ def measure_precision(dev, st, spins, flush) -> dict:
     return out
 
 
+def measure_extensions(args, dev, st, spins, flush) -> dict:
+    """The rows beyond the amplitude: the per-sample Jacobian of log|psi_P| (16x16, 1024
+    configurations x 8 images, benchmark weights), the BCS-backflow ansatz on the benchmark's
+    8192 configurations x 8 images (throughput of the chosen CNN form, and its |delta log|psi_P||
+    against the BCS all-FP64 form), and the packed observables (transverse spin at one
+    reference site, the d-wave F and G families at R = (0, 0)) on 1024 configurations."""
+    import torch
+
+    import neuralhubbard_b200 as nh
+    from neuralhubbard_b200 import _lib
+    from neuralhubbard_b200.observables import PackedDwave, transverse_terms
+
+    out = {}
+    params = nh.init_params(L, L, CHANNELS, LAYERS, std=0.02, seed=0)
+    model = nh.PfaffianBackflow(L, L, NE, NE, params=params, device=dev)
+    state = nh.Variational(model, symm=True, max_parallel=1024)
+    sj = spins[:1024]
+    state.jacobian(sj)
+    torch.cuda.synchronize()
+    _lib.profile_read()
+    _lib.profile_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(2):
+        psi, J = state.jacobian(sj)
+    e1.record(st)
+    torch.cuda.synchronize()
+    _lib.profile_enable(False)
+    kern = _lib.profile_read()
+    ms = e0.elapsed_time(e1) / 2
+    out["jacobian"] = {"lattice": "16x16", "configurations": 1024, "images": 8,
+                       "parameters": int(J.shape[1]), "ms_per_call": ms,
+                       "samples_per_s": 1024 / (ms / 1e3),
+                       "kernels_ms_per_call": {k: v[0] / 2 for k, v in kern.items()}}
+    del J, psi
+    # BCS ansatz
+    bp = dict(params)
+    bp["W"] = params["W"][0]
+    bp["delta_d"] = 0.1
+    bcs = {}
+    ref = None
+    for name, kw in (("all FP64 (cond_tau 1, reference)", dict(cond_tau=1.0)),
+                     ("chosen (defaults): tcgen05 BF16x3 CNN", dict(cnn_mode=2)),
+                     ("plain (defaults): FP32 CNN", dict(cnn_mode=0))):
+        m = nh.BCSBackflow(L, L, NE, NE, params=bp, device=dev, **kw)
+        sb = nh.Variational(m, symm=True, max_parallel=BATCH)
+        bms, bk = time_amplitudes(sb, spins, 3, 1, flush, st, True)
+        ps = sb(spins)
+        sg, la = ps.sign.cpu().numpy(), ps.logabs.cpu().numpy()
+        if ref is None:
+            ref = (sg, la)
+        bcs[name] = {"amplitudes_per_s": BATCH * IMAGES / (bms / 3 / 1e3),
+                     "kernels_ms_per_step": {k: v[0] / 3 for k, v in bk.items()},
+                     **_err_stats(la, ref[1], sg, ref[0])}
+        del m, sb, ps
+    out["bcs"] = {"lattice": "16x16", "configurations": BATCH, "images": IMAGES,
+                  "n_up x n_dn": f"{NE} x {NE}", "delta_d": 0.1, "forms": bcs}
+    # packed observables
+    so = spins[:1024]
+    samples = nh.Samples(so, state(so))
+    transverse_terms(state, samples, (0, 0))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    T = transverse_terms(state, samples, (0, 0))
+    torch.cuda.synchronize()
+    t_tr = time.perf_counter() - t0
+    dw = PackedDwave(L, L, R=(0, 0))
+    t0 = time.perf_counter()
+    F, G = dw.measure(state, samples)
+    t_dw = time.perf_counter() - t0
+    out["observables"] = {
+        "lattice": "16x16", "configurations": 1024, "projected": True,
+        "transverse_spin_s": t_tr, "transverse_terms": int(T.numel()),
+        "dwave_s": t_dw, "dwave_F_terms": len(F), "dwave_G_terms": len(G),
+        "sum_rule_Sz0": float(T[0, 0].item() + T[1, 0].item()),
+        "note": "wall-clock seconds of one call each (each call reads its connection count back "
+                "once); the terms' connections run through the amplitude pipeline"}
+    return out
+
+
 def measure_large(args, dev, st, q) -> dict:
     """Config 5 shapes: Metropolis at 32x32 (n = 896, large-lattice path) with 4096 chains x 8
     images, uniform hop against the learned proposal (the 16x16-trained weights: the proposal
@@ -876,6 +958,9 @@ def run_ours(args) -> None:
     resconv = None
     if world == 1 and not args.no_resconv:
         resconv = measure_resconv(args, dev, st)
+    extensions = None
+    if world == 1 and not args.no_extensions:
+        extensions = measure_extensions(args, dev, st, spins, flush)
     released_sampling = None
     if world == 1 and args.released_sampling:
         released_sampling = measure_released_sampling(args, dev, st)
@@ -913,6 +998,7 @@ def run_ours(args) -> None:
             "precision": precision,
             "resconv": resconv,
             "released_sampling": released_sampling,
+            "extensions": extensions,
             "roofline": roof, "kernels": kernels, "gpu_launches": launches,
             "cpu_baseline": cpu, "clocks": clk,
         }
@@ -1172,6 +1258,8 @@ def main():
                     help="skip the 32x32 (n = 896) Metropolis measurement")
     ap.add_argument("--large-chains", type=int, default=4096)
     ap.add_argument("--large-steps", type=int, default=2)
+    ap.add_argument("--no-extensions", action="store_true",
+                    help="skip the Jacobian, BCS and packed-observable blocks")
     ap.add_argument("--no-resconv", action="store_true",
                     help="skip the released-state residual network block")
     ap.add_argument("--released-sampling", action="store_true",
