@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define NH_ABI_VERSION 9
+#define NH_ABI_VERSION 10
 
 enum {
   NH_OK = 0,
@@ -396,8 +396,10 @@ int nh_proposal_sample(const int8_t* spins, int batch, const nh_proposal_params*
                        float* log_q_ratio, void* stream);
 /* Training: loss = -(1/batch) sum_b weights[b] log q(moves[b] | spins[b]) (records whose move
  * is not valid contribute nothing) into loss (1,) and its gradient (NH_PROPOSAL_PARAMS,) into
- * grad, both FP32, summed in a fixed order (deterministic). */
-size_t nh_proposal_backward_workspace_bytes(int batch);
+ * grad, both FP32, summed in a fixed order (deterministic).  The workspace holds per-CTA
+ * gradient partials and, for lattices whose activation planes exceed shared memory (more than 559
+ * sites, e.g. 24x24 and 32x32), per-CTA planes (about 100 MB at 32x32). */
+size_t nh_proposal_backward_workspace_bytes(int batch, const nh_proposal_params* q);
 int nh_proposal_backward(const int8_t* spins, const int32_t* moves, const float* weights,
                          int batch, const nh_proposal_params* q, float* loss, float* grad,
                          void* workspace, size_t workspace_bytes, void* stream);

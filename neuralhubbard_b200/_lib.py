@@ -19,7 +19,7 @@ ANSATZ_PFAFFIAN, ANSATZ_BCS = 0, 1
 OBS_TRANSVERSE_SPIN, OBS_PAIR, OBS_HOP = 0, 1, 2
 FLAG_ZERO_PIVOT, FLAG_NONFINITE, FLAG_GROWTH, FLAG_REFINED, FLAG_CANCEL = 1, 2, 4, 8, 16
 FLAG_TIMEOUT = 32
-ABI_VERSION = 9
+ABI_VERSION = 10
 
 c_void_p, c_int, c_int64, c_uint64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64
 c_float, c_double, c_size_t = ctypes.c_float, ctypes.c_double, ctypes.c_size_t
@@ -110,7 +110,7 @@ SIGNATURES = {
     "nh_proposal_forward": (c_int, [c_void_p, c_int, P_Q, c_void_p, c_void_p]),
     "nh_proposal_sample": (c_int, [c_void_p, c_int, P_Q, c_uint64, c_int64, c_void_p, c_void_p,
                                    c_void_p, c_void_p, c_void_p]),
-    "nh_proposal_backward_workspace_bytes": (c_size_t, [c_int]),
+    "nh_proposal_backward_workspace_bytes": (c_size_t, [c_int, P_Q]),
     "nh_proposal_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, P_Q, c_void_p,
                                      c_void_p, c_void_p, c_size_t, c_void_p]),
     "nh_proposal_adam_step": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int64,

@@ -267,6 +267,13 @@ size_t prop_backward_smem(int N) {
          2 * N + 16;
 }
 
+// Shared memory of the global-plane variant (weights, scratch and the configuration).
+size_t prop_backward_smem_gact(int N) {
+  return sizeof(float) * ((size_t)kPCount + kPBwd + kPL1Scratch + 64) + 2 * N + 16;
+}
+
+size_t prop_plane_floats(int N) { return (size_t)(2 + 5 * kPC) * (N + 1); }
+
 __global__ void __launch_bounds__(kPThreads) prop_sample_kernel(
     const int8_t* __restrict__ spins, int batch, const __nv_bfloat16* __restrict__ wg, int Lx,
     int Ly, int n_dirs, uint32_t k0, uint32_t k1, uint32_t step_lo, uint32_t step_hi,
@@ -403,10 +410,14 @@ __global__ void __launch_bounds__(kPThreads) prop_logits_kernel(
 }
 
 // Loss -(1/B) sum_b w_b log q(m_b | s_b) and its gradient; per-CTA partials (grid, kPCount + 1).
+// GACT: the activation planes (x0, a1, g1, a2, g2, z: (2 + 5 kPC) NS floats) live in a per-CTA
+// slice of global memory (plane_scratch) for lattices whose planes exceed shared memory; the
+// weights and the reduction scratch stay in shared memory.
+template <bool GACT>
 __global__ void __launch_bounds__(kPThreads, 1) prop_backward_kernel(
     const int8_t* __restrict__ spins, const int32_t* __restrict__ moves,
     const float* __restrict__ weights, int batch, const __nv_bfloat16* __restrict__ wg, int Lx,
-    int Ly, int n_dirs, float inv_batch, float* __restrict__ part) {
+    int Ly, int n_dirs, float inv_batch, float* __restrict__ part, float* plane_scratch) {
   extern __shared__ __align__(16) float psm[];
   const int N = Lx * Ly, NS = N + 1, M = kPC * N;
   const int tid = threadIdx.x;
@@ -414,13 +425,13 @@ __global__ void __launch_bounds__(kPThreads, 1) prop_backward_kernel(
   float* wb = wf + kPCount;
   float* l1s = wb + kPBwd;  // layer-1 partials
   float* red = l1s + kPL1Scratch;
-  float* x0 = red + 64;
+  float* x0 = GACT ? plane_scratch + (size_t)blockIdx.x * (2 + 5 * kPC) * NS : red + 64;
   float* a1 = x0 + 2 * NS;
   float* g1 = a1 + kPC * NS;
   float* a2 = g1 + kPC * NS;
   float* g2 = a2 + kPC * NS;
   float* z = g2 + kPC * NS;
-  int8_t* s_sh = reinterpret_cast<int8_t*>(z + kPC * NS);
+  int8_t* s_sh = reinterpret_cast<int8_t*>(GACT ? red + 64 : z + kPC * NS);
   stage_prop_weights(wg, wf, wb);
   const int co = tid >> 4, ci = tid & 15;       // pair of layers 2 and 3
   const int p1 = tid & 31, grp = tid >> 5;      // pair and site group of layer 1
@@ -593,6 +604,10 @@ size_t proposal_backward_parts(int batch) {
   return (size_t)std::max(1, std::min(batch, kPMaxParts));
 }
 
+constexpr int kPGactPerSm = 2;  // CTAs per SM of the global-plane backward (its scratch slices)
+
+bool prop_backward_gact(int N) { return prop_backward_smem(N) > kSmemLimit; }
+
 }  // namespace nh
 
 using namespace nh;
@@ -637,8 +652,14 @@ int nh_proposal_sample(const int8_t* spins, int batch, const nh_proposal_params*
                             static_cast<cudaStream_t>(stream));
 }
 
-size_t nh_proposal_backward_workspace_bytes(int batch) {
-  return proposal_backward_parts(batch) * (kPCount + 1) * sizeof(float);
+size_t nh_proposal_backward_workspace_bytes(int batch, const nh_proposal_params* q) {
+  size_t bytes = proposal_backward_parts(batch) * (kPCount + 1) * sizeof(float);
+  if (q && prop_backward_gact(q->Lx * q->Ly)) {
+    const size_t slices = std::min<size_t>(proposal_backward_parts(batch),
+                                           (size_t)kPGactPerSm * num_sms());
+    bytes = ((bytes + 255) & ~(size_t)255) + slices * prop_plane_floats(q->Lx * q->Ly) * 4;
+  }
+  return bytes;
 }
 
 int nh_proposal_backward(const int8_t* spins, const int32_t* moves, const float* weights,
@@ -648,24 +669,37 @@ int nh_proposal_backward(const int8_t* spins, const int32_t* moves, const float*
   if (rc) return rc;
   if (!spins || !moves || !weights || !grad || batch <= 0)
     return fail(NH_ERR_INVALID, "proposal_backward: buffers");
-  const size_t need = nh_proposal_backward_workspace_bytes(batch);
+  const size_t need = nh_proposal_backward_workspace_bytes(batch, q);
   if ((rc = check_workspace(workspace, workspace_bytes, need, "proposal_backward"))) return rc;
-  const size_t smem = prop_backward_smem(q->Lx * q->Ly);
-  if (smem > kSmemLimit)
-    return fail(NH_ERR_UNSUPPORTED, "proposal_backward: %d sites exceed shared memory",
-                q->Lx * q->Ly);
-  if ((rc = prop_smem_attr(prop_backward_kernel, smem, &g_backward_smem))) return rc;
-  int grid = 0;
-  if ((rc = prop_grid(prop_backward_kernel, smem, batch, &grid))) return rc;
-  grid = std::min<int>(grid, (int)proposal_backward_parts(batch));
+  const int N = q->Lx * q->Ly;
+  const bool gact = prop_backward_gact(N);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   float* part = static_cast<float*>(workspace);
-  {
+  int grid = 0;
+  if (!gact) {
+    const size_t smem = prop_backward_smem(N);
+    if ((rc = prop_smem_attr(prop_backward_kernel<false>, smem, &g_backward_smem))) return rc;
+    if ((rc = prop_grid(prop_backward_kernel<false>, smem, batch, &grid))) return rc;
+    grid = std::min<int>(grid, (int)proposal_backward_parts(batch));
     ProfScope prof_scope(NH_K_PROP_BACKWARD, st);
-    prop_backward_kernel<<<grid, kPThreads, smem, st>>>(
+    prop_backward_kernel<false><<<grid, kPThreads, smem, st>>>(
         spins, moves, weights, batch, static_cast<const __nv_bfloat16*>(q->weights), q->Lx,
-        q->Ly, q->n_dirs, 1.0f / (float)batch, part);
+        q->Ly, q->n_dirs, 1.0f / (float)batch, part, nullptr);
     if ((rc = check_launch("prop_backward_kernel"))) return rc;
+  } else {
+    const size_t smem = prop_backward_smem_gact(N);
+    static size_t g_gact_smem = 48 * 1024;
+    if ((rc = prop_smem_attr(prop_backward_kernel<true>, smem, &g_gact_smem))) return rc;
+    grid = (int)std::min<size_t>(proposal_backward_parts(batch),
+                                 (size_t)kPGactPerSm * num_sms());
+    const size_t part_bytes = proposal_backward_parts(batch) * (kPCount + 1) * sizeof(float);
+    float* planes = reinterpret_cast<float*>(static_cast<char*>(workspace) +
+                                             ((part_bytes + 255) & ~(size_t)255));
+    ProfScope prof_scope(NH_K_PROP_BACKWARD, st);
+    prop_backward_kernel<true><<<grid, kPThreads, smem, st>>>(
+        spins, moves, weights, batch, static_cast<const __nv_bfloat16*>(q->weights), q->Lx,
+        q->Ly, q->n_dirs, 1.0f / (float)batch, part, planes);
+    if ((rc = check_launch("prop_backward_kernel<global planes>"))) return rc;
   }
   prop_reduce_kernel<<<(kPCount + 256) / 256, 256, 0, st>>>(part, grid, grad, loss);
   return check_launch("prop_reduce_kernel");

@@ -102,9 +102,9 @@ class HopProposal:
         B = spins.shape[0]
         loss = torch.empty(1, dtype=torch.float32, device=self.device)
         grad = torch.empty(PARAM_COUNT, dtype=torch.float32, device=self.device)
-        nbytes = _lib.load().nh_proposal_backward_workspace_bytes(B)
-        ws = workspace(nbytes, self.device, "proposal_backward")
         q = self.c_params()
+        nbytes = _lib.load().nh_proposal_backward_workspace_bytes(B, ctypes.byref(q))
+        ws = workspace(nbytes, self.device, "proposal_backward")
         _lib.call("nh_proposal_backward", spins.data_ptr(), moves.data_ptr(), weights.data_ptr(),
                   B, ctypes.byref(q), loss.data_ptr(), grad.data_ptr(), ws.data_ptr(), ws.numel(),
                   stream_ptr(self.device))

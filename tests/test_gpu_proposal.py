@@ -34,8 +34,10 @@ def test_logits_vs_oracle(L, ne):
     assert np.max(np.abs(z - z0)) < 1e-4 * max(1.0, np.abs(z0).max())
 
 
-@pytest.mark.parametrize("L,ne,n_dirs", [(6, 10, 8), (8, 28, 4)])
+@pytest.mark.parametrize("L,ne,n_dirs", [(6, 10, 8), (8, 28, 4), (24, 252, 8), (32, 448, 8)])
 def test_loss_and_gradient_vs_oracle(L, ne, n_dirs):
+    """24x24 and 32x32 exceed shared memory: the backward keeps its activation planes in
+    per-CTA global slices of the workspace."""
     q, th = make_proposal(L, seed=2, n_dirs=n_dirs)
     rng = np.random.default_rng(5)
     s = olat.random_configs(rng, 12, L * L, ne, ne)
