@@ -694,6 +694,81 @@ def measure_large(args, dev, st, q) -> dict:
     return out
 
 
+def measure_config5(args, dev, st) -> dict:
+    """Config 5 at 32x32 (n = 896): the learned proposal trained at 32x32 on records of plain
+    chains, against the uniform hop.  Reduced from the stated 4096 chains, 2^20 records and a
+    tau_int over >= 50 tau to what one GPU does in minutes (a projected 32x32 amplitude costs
+    ~0.7 ms): ``c5_chains`` chains equilibrated by ``c5_burn`` plain steps, ``c5_records``
+    training records (Barker weight) from their last configurations, 2000 Adam steps, then
+    ``c5_steps`` measured steps per sampler from the same start; tau_int of log|psi| with its
+    chain-group error, effective samples/s, and E/N on 16 final configurations each."""
+    import torch
+
+    import neuralhubbard_b200 as nh
+    from neuralhubbard_b200 import stats
+
+    Lk = 32
+    Nk = Lk * Lk
+    nek = 7 * Nk // 16
+    B, burn, steps = args.c5_chains, args.c5_burn, args.c5_steps
+    params = nh.init_params(Lk, Lk, CHANNELS, LAYERS, std=0.02, seed=0)
+    model = nh.PfaffianBackflow(Lk, Lk, nek, nek, params=params, device=dev)
+    state = nh.Variational(model, symm=True, max_parallel=4096)
+    init = nh.random_spins(np.random.default_rng(51), B, Nk, nek, nek)
+    eq = nh.ParticleHop(state, B, n_neighbor=(1, 2), initial_spins=init, seed=52)
+    n_snap = max(1, min(burn, args.c5_records // B))
+    t0 = time.perf_counter()
+    eq.run(burn - n_snap)
+    snaps = []
+    for _ in range(n_snap):
+        eq.run(1)
+        snaps.append(eq.spins.clone())
+    torch.cuda.synchronize()
+    t_burn = time.perf_counter() - t0
+    start = eq.spins.clone()
+    t0 = time.perf_counter()
+    rec = nh.training_records(state, torch.cat(snaps), seed=53, weight="barker")
+    torch.cuda.synchronize()
+    t_rec = time.perf_counter() - t0
+    del snaps
+    q = nh.HopProposal(Lk, Lk, 8, seed=54, std=0.05, device=dev)
+    t0 = time.perf_counter()
+    losses = q.train(rec, args.train_steps, batch=512, lr=3e-3, seed=55)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    out = {"lattice": "32x32", "pfaffian_n": 2 * nek, "chains": B, "burn_in_steps": burn,
+           "burn_in_seconds": t_burn, "measured_steps": steps,
+           "proposal_training": {"records": int(rec[0].shape[0]), "steps": args.train_steps,
+                                 "batch": 512, "target": "barker r/(1+r)",
+                                 "record_seconds": t_rec, "train_seconds": t_train,
+                                 "loss_first": float(np.mean(losses[:20])),
+                                 "loss_last": float(np.mean(losses[-20:]))}}
+    del rec
+    H = nh.Hubbard(8.0, [1.0, -0.2], [1, 2])
+    for name, make in (("uniform_hop", lambda: nh.ParticleHop(state, B, n_neighbor=(1, 2),
+                                                              initial_spins=start, seed=56)),
+                       ("learned", lambda: nh.LearnedHop(state, B, q, initial_spins=start,
+                                                         seed=57))):
+        smp = make()
+        series, ms, acc = run_chains(smp, steps, st)
+        te = stats.tau_int_error(series)
+        tau = te["tau"]
+        err = te["err_groups"] if te["err_groups"] is not None else te["err_sokal"]
+        rate = stats.effective_rate(B, steps, tau, ms / 1e3)
+        e = H.Oloc(state, nh.Samples(smp.spins[:16].contiguous(), smp.psi[:16]))
+        e = e.cpu().numpy() / Nk
+        out[name] = {"acceptance": acc, "tau_int_logpsi": tau, "tau_int_logpsi_err": err,
+                     "tau_window": te["window"], "ms_per_step": ms / steps,
+                     "effective_samples_per_s": rate,
+                     "effective_samples_per_s_err": rate * err / tau,
+                     "energy_per_site": float(e.mean()),
+                     "energy_per_site_err": float(e.std(ddof=1) / np.sqrt(16))}
+        del smp
+    out["learned_vs_uniform"] = (out["learned"]["effective_samples_per_s"]
+                                 / out["uniform_hop"]["effective_samples_per_s"])
+    return out
+
+
 def measure_resconv(args, dev, st) -> dict:
     """The released states' residual network (16 blocks x 64 channels, d = 32) at 16x16: projected
     amplitudes of 1024 configurations x 8 images on CUDA cores (FP32) and on the tensor cores
@@ -958,6 +1033,9 @@ def run_ours(args) -> None:
     resconv = None
     if world == 1 and not args.no_resconv:
         resconv = measure_resconv(args, dev, st)
+    config5 = None
+    if world == 1 and args.config5:
+        config5 = measure_config5(args, dev, st)
     extensions = None
     if world == 1 and not args.no_extensions:
         extensions = measure_extensions(args, dev, st, spins, flush)
@@ -999,6 +1077,7 @@ def run_ours(args) -> None:
             "resconv": resconv,
             "released_sampling": released_sampling,
             "extensions": extensions,
+            "config5": config5,
             "roofline": roof, "kernels": kernels, "gpu_launches": launches,
             "cpu_baseline": cpu, "clocks": clk,
         }
@@ -1258,6 +1337,12 @@ def main():
                     help="skip the 32x32 (n = 896) Metropolis measurement")
     ap.add_argument("--large-chains", type=int, default=4096)
     ap.add_argument("--large-steps", type=int, default=2)
+    ap.add_argument("--config5", action="store_true",
+                    help="the learned proposal trained and measured at 32x32 (several minutes)")
+    ap.add_argument("--c5-chains", type=int, default=512)
+    ap.add_argument("--c5-burn", type=int, default=200)
+    ap.add_argument("--c5-steps", type=int, default=300)
+    ap.add_argument("--c5-records", type=int, default=65536)
     ap.add_argument("--no-extensions", action="store_true",
                     help="skip the Jacobian, BCS and packed-observable blocks")
     ap.add_argument("--no-resconv", action="store_true",
