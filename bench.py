@@ -1134,6 +1134,8 @@ def run_reference(args) -> None:
 #   amplitude_plain    the same on the plain form (fused FP32 CNN + Pfaffian kernel)
 #   jacobian           16x16 per-sample Jacobian of log|psi_P|, 128 x 8 images (Pfaffian adjoint,
 #                      pairing VJP and CNN VJP kernels after the amplitude pipeline)
+#   bcs                16x16 BCS-backflow projected amplitudes, 256 x 8 images (determinant kernels)
+#   observables        16x16 transverse-spin terms of one reference site, 128 configurations
 
 def _model(L, cnn_mode=0):
     import neuralhubbard_b200 as nh
@@ -1301,11 +1303,42 @@ def case_jacobian(repeat):
         state.jacobian(s)
 
 
+def case_bcs(repeat):
+    import torch
+
+    import neuralhubbard_b200 as nh
+
+    ne = 112
+    params = nh.init_params(16, 16, 32, 4, std=0.02, seed=0)
+    params["W"] = params["W"][0]
+    params["delta_d"] = 0.1
+    model = nh.BCSBackflow(16, 16, ne, ne, params=params, cnn_mode=2)
+    state = nh.Variational(model, symm=True)
+    s = torch.from_numpy(nh.random_spins(np.random.default_rng(11), 256, 256, ne, ne)).cuda()
+    for _ in range(repeat):
+        state(s)
+
+
+def case_observables(repeat):
+    import torch
+
+    import neuralhubbard_b200 as nh
+    from neuralhubbard_b200.observables import transverse_terms
+
+    model, ne = _model(16, cnn_mode=2)
+    state = nh.Variational(model, symm=True)
+    s = torch.from_numpy(nh.random_spins(np.random.default_rng(12), 128, 256, ne, ne)).cuda()
+    samples = nh.Samples(s, state(s))
+    for _ in range(repeat):
+        transverse_terms(state, samples, (0, 0))
+
+
 CASES = {"pairing": case_pairing, "hops": case_hops, "eloc": case_eloc,
          "proposal_sample": case_proposal_sample, "proposal_backward": case_proposal_backward,
          "resconv_tc": case_resconv_tc, "resconv": case_resconv,
          "refine": case_refine, "amplitude": case_amplitude,
-         "amplitude_plain": case_amplitude_plain, "jacobian": case_jacobian}
+         "amplitude_plain": case_amplitude_plain, "jacobian": case_jacobian,
+         "bcs": case_bcs, "observables": case_observables}
 
 
 
