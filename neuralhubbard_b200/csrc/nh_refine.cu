@@ -263,7 +263,9 @@ size_t features_smem(int N, int C, int Lx, int elt) {
   return ((act + 15) & ~(size_t)15) + (size_t)elt * ((size_t)C * C * 9 + C);
 }
 
-template <int D>
+// MODE is a.mode as a template argument, so that each instance holds only its own phase-1 code
+// (the register allocation of the elimination is then not shaped by the other modes).
+template <int D, int MODE>
 __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int perm_s[kRefineMaxN];
@@ -282,7 +284,7 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
     for (int p = tid; p < n; p += kRThreads) perm_s[p] = pr[p];
     __syncthreads();
     // Phases 1 and 2: the permuted lower triangle in FP64 shared memory.
-    if (a.mode == 0) {
+    if constexpr (MODE == 0) {
       const float* F = a.F + (size_t)item * n * n;
       for (int p = wid; p < n; p += kRWarps) {
         const int i = perm_s[p];
@@ -295,11 +297,11 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
     } else {
       const int tot = tri_elems(n);  // a multiple of 4
       unsigned char* slb = static_cast<unsigned char*>(a.slice) + (size_t)blockIdx.x * slice_stride(n, D);
-      if (a.mode == 1 || a.mode == 3) {
+      if constexpr (MODE == 1 || MODE == 3) {
         float* sl = reinterpret_cast<float*>(slb);
         const float* Yg = static_cast<const float*>(a.Y) + (size_t)item * n * D;
         const int32_t* ig = a.idx + (size_t)item * n;
-        if (a.mode == 3) {  // the item's FP32 features, rows and modes to the slice
+        if constexpr (MODE == 3) {  // the item's FP32 features, rows and modes to the slice
           features_to(a, item, smem, sl, reinterpret_cast<int32_t*>(sl + n * D));
           Yg = sl;
           ig = reinterpret_cast<const int32_t*>(sl + n * D);
@@ -311,7 +313,7 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
         double* sl = reinterpret_cast<double*>(slb);
         const double* Yg = static_cast<const double*>(a.Y) + (size_t)slot * n * D;
         const int32_t* ig = a.idx + (size_t)slot * n;
-        if (a.mode == 4) {
+        if constexpr (MODE == 4) {
           features_to(a, item, smem, sl, reinterpret_cast<int32_t*>(sl + n * D));
           Yg = sl;
           ig = reinterpret_cast<const int32_t*>(sl + n * D);
@@ -520,18 +522,21 @@ int launch_refine_d(RefineArgs a, int max_slots, cudaStream_t st) {
   }
   if (smem > kRefineSmemLimit)
     return fail(NH_ERR_UNSUPPORTED, "refine: n=%d needs %zu B of shared memory", a.n, smem);
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(
-        refine_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRefineSmemLimit);
+  static bool configured[5] = {false, false, false, false, false};
+  auto kern = a.mode == 0 ? refine_kernel<D, 0> : a.mode == 1 ? refine_kernel<D, 1>
+            : a.mode == 2 ? refine_kernel<D, 2> : a.mode == 3 ? refine_kernel<D, 3>
+                                                 : refine_kernel<D, 4>;
+  if (!configured[a.mode]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kRefineSmemLimit);
     if (e != cudaSuccess) return check_cuda(e, "refine smem attribute");
-    configured = true;
+    configured[a.mode] = true;
   }
   int grid = num_sms();
   if (grid > max_slots) grid = max_slots;
   if (grid <= 0) return NH_OK;
   ProfScope prof_scope(NH_K_REFINE, st);
-  refine_kernel<D><<<grid, kRThreads, smem, st>>>(a);
+  kern<<<grid, kRThreads, smem, st>>>(a);
   return check_launch("refine_kernel");
 }
 
@@ -545,6 +550,7 @@ int launch_refine(const RefineLaunch& q, cudaStream_t st) {
   if (q.n <= 0 || q.n % 2 || q.n > kRefineMaxN)
     return fail(NH_ERR_UNSUPPORTED, "refine: n=%d (even, <= %d)", q.n, kRefineMaxN);
   if (q.max_slots <= 0) return NH_OK;
+  if (q.mode < 0 || q.mode > 4) return fail(NH_ERR_INVALID, "refine: mode %d", q.mode);
   if (q.mode != 0 && !q.slice) return fail(NH_ERR_INVALID, "refine: gather mode needs the slice");
   RefineArgs a{};
   a.n = q.n;
