@@ -237,3 +237,50 @@ def test_timeout_flag_raises():
 
     with pytest.raises(_lib.DeviceTimeoutError):
         _lib.check_flags(torch.from_numpy(bad), "test")
+
+
+def test_new_entry_points_validate_arguments_without_a_gpu():
+    """The backward, BCS and observable entry points reject bad arguments before any device
+    work (status codes and nh_last_error; no CUDA call is made)."""
+    import ctypes
+
+    from neuralhubbard_b200 import _lib
+
+    lib = _lib.load()
+    p8 = ctypes.c_void_p(4096)
+    assert lib.nh_pfaffian_adjoint(p8, 7, 4, p8, None, None) == -2  # odd n
+    assert lib.nh_pfaffian_adjoint(p8, 226, 4, p8, None, None) == -2  # beyond 224
+    assert lib.nh_pfaffian_adjoint(None, 8, 4, p8, None, None) == -1
+    assert lib.nh_pairing_occ_vjp(p8, p8, p8, p8, 24, 24, 16, 100, 2, p8, p8, None) == -2
+
+    def prm(**kw):
+        f = dict(conv_w=4096, conv_b=4096, conv_w_packed=4096, conv_w_tc=4096, Wt=4096,
+                 Wt64=4096, Lx=8, Ly=8, n_up=28, n_dn=28, channels=32, layers=4, cnn_mode=0,
+                 pf_mode=0, net=_lib.NET_CNN, ansatz=_lib.ANSATZ_PFAFFIAN, cond_tau=5.0,
+                 cancel_tau=8.0, refine_tau=0.0, delta_d=0.0)
+        f.update(kw)
+        return _lib.BackflowParams(**f)
+
+    p = prm()
+    assert lib.nh_param_count(ctypes.byref(p)) == (32 * 2 * 9 + 32) + 3 * (32 * 32 * 9 + 32) \
+        + 3 * 64 * 16 + 1
+    assert lib.nh_param_count(ctypes.byref(prm(net=_lib.NET_RESCONV))) == 0
+    bcs = prm(ansatz=_lib.ANSATZ_BCS)
+    rc = lib.nh_log_jacobian(p8, 4, 8, ctypes.byref(bcs), p8, 0.55, p8, p8, p8, None, p8,
+                             1 << 30, None)
+    assert rc == -2 and b"log_jacobian" in lib.nh_last_error()
+    rc = lib.nh_log_jacobian(p8, 4, 3, ctypes.byref(p), p8, 0.55, p8, p8, p8, None, p8, 1 << 30,
+                             None)
+    assert rc == -1  # n_symm must be 1 or 8
+
+    def obs(kind, a0, a1, **kw):
+        q = prm(**kw)
+        return lib.nh_observable(p8, p8, p8, 4, 8, ctypes.byref(q), kind, a0, a1, p8, p8,
+                                 1 << 30, None)
+
+    assert obs(7, 0, 0) == -1 and b"kind 7" in lib.nh_last_error()
+    assert obs(_lib.OBS_TRANSVERSE_SPIN, 64, 0) == -1  # site beyond the 8x8 lattice
+    assert obs(_lib.OBS_PAIR, 3, -1) == -1
+    assert obs(_lib.OBS_HOP, 3, 2) == -1  # spin must be 0 or 1
+    assert lib.nh_observable_workspace_bytes(4, 8, 9, ctypes.byref(p)) == 0
+    assert lib.nh_observable_workspace_bytes(4, 8, _lib.OBS_PAIR, ctypes.byref(p)) > 0
