@@ -38,8 +38,10 @@ struct CnnArgs {
 
 // GACT: the two activation planes live in a per-CTA slice of global memory (large lattices,
 // where they exceed shared memory); shared memory then holds the weights and scratch only.
-template <typename T, bool GACT = false>
-__global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
+// TH: threads per CTA; the FP64 instance with resident planes runs 512 (one CTA per SM: its
+// planes and weights take ~210 KB), so that twice the warps hide the FP64 latency.
+template <typename T, bool GACT = false, int TH = kNumThreads>
+__global__ void __launch_bounds__(TH) cnn_kernel(CnnArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = a.N, C = a.C, NS = N + 1, M2 = 2 * N;
   const int tid = threadIdx.x;
@@ -70,12 +72,12 @@ __global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
     const int8_t* base = a.cl.spins + (int64_t)smp * M2;
 
     __syncthreads();  // previous item's readers of simg/act are done
-    const T* in = cnn_layers<T>(a.wp, a.b, a.Lx, a.Ly, C, a.layers, base, fr, to, g, actA, actB,
-                                wsm, bsm, simg);
+    const T* in = cnn_layers<T, TH>(a.wp, a.b, a.Lx, a.Ly, C, a.layers, base, fr, to, g, actA,
+                                    actB, wsm, bsm, simg);
     const int d = C / 2;
     if (a.mode == 0) {
       float* dst = a.feat + (int64_t)item * C * N;
-      for (int o = tid; o < C * N; o += kNumThreads) {
+      for (int o = tid; o < C * N; o += TH) {
         const int aa = o % d;
         const int site = (o / d) % N;
         const int sg = o / (N * d);
@@ -83,10 +85,11 @@ __global__ void __launch_bounds__(kNumThreads) cnn_kernel(CnnArgs<T> a) {
       }
       continue;
     }
-    write_occupied_rows(simg, occl, wbuf, N, a.n, d, g, a.Lx, a.Ly,
-                        a.Y + (int64_t)slot * a.n * d, a.idx + (int64_t)slot * a.n,
-                        a.item_sign + item,
-                        [&](int sg, int aa, int site) { return in[(sg * d + aa) * NS + site]; });
+    auto feat_of = [&](int sg, int aa, int site) { return in[(sg * d + aa) * NS + site]; };
+    write_occupied_rows<T, decltype(feat_of), TH>(simg, occl, wbuf, N, a.n, d, g, a.Lx, a.Ly,
+                                                  a.Y + (int64_t)slot * a.n * d,
+                                                  a.idx + (int64_t)slot * a.n,
+                                                  a.item_sign + item, feat_of);
   }
 }
 
@@ -124,7 +127,7 @@ int launch_pack_cnn(const float* conv_w, int channels, int layers, float* packed
   return check_launch("pack_kernel");
 }
 
-template <typename T, bool GACT>
+template <typename T, bool GACT, int TH = kNumThreads>
 int launch_cnn_t(const CnnLaunch& q, int N, int C, cudaStream_t st) {
   const nh_backflow_params& p = *q.p;
   const size_t smem = cnn_smem<T, GACT>(N, C);
@@ -135,11 +138,12 @@ int launch_cnn_t(const CnnLaunch& q, int N, int C, cudaStream_t st) {
     return fail(NH_ERR_UNSUPPORTED, "cnn: N=%d needs the large-lattice activation scratch", N);
   const int slots = q.slot_item ? q.max_slots : q.cl->n_cfg * q.cl->G;
   if (slots <= 0) return NH_OK;
-  int grid = GACT ? num_sms() * kCnnBigPerSm : num_sms() * (smem > 113 * 1024 ? 1 : 2) * 4;
+  int grid = GACT ? num_sms() * kCnnBigPerSm
+                  : num_sms() * (smem > 113 * 1024 || TH > kNumThreads ? 1 : 2) * 4;
   if (grid > slots) grid = slots;
   static size_t configured = 0;
   if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(cnn_kernel<T, GACT>,
+    cudaError_t e = cudaFuncSetAttribute(cnn_kernel<T, GACT, TH>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return check_cuda(e, "cnn smem attribute");
     configured = smem;
@@ -148,7 +152,7 @@ int launch_cnn_t(const CnnLaunch& q, int N, int C, cudaStream_t st) {
                p.n_up + p.n_dn, q.mode, q.slot_item, q.slot_count, q.max_slots,
                q.feat, static_cast<T*>(q.Y), q.idx, q.item_sign, static_cast<T*>(q.act)};
   ProfScope prof_scope(sizeof(T) == 8 ? NH_K_CNN64 : NH_K_CNN, st);
-  cnn_kernel<T, GACT><<<grid, kNumThreads, smem, st>>>(a);
+  cnn_kernel<T, GACT, TH><<<grid, TH, smem, st>>>(a);
   return check_launch(sizeof(T) == 8 ? "cnn_kernel<double>" : "cnn_kernel<float>");
 }
 
@@ -167,7 +171,7 @@ int launch_cnn(const CnnLaunch& q, cudaStream_t st) {
   if (!p.conv_w_packed)
     return fail(NH_ERR_INVALID, "cnn: conv_w_packed is null (call nh_pack_cnn_weights)");
   if (q.fp64)
-    return cnn_smem<double>(N, C) <= 227 * 1024 ? launch_cnn_t<double, false>(q, N, C, st)
+    return cnn_smem<double>(N, C) <= 227 * 1024 ? launch_cnn_t<double, false, 512>(q, N, C, st)
                                                  : launch_cnn_t<double, true>(q, N, C, st);
   return cnn_smem<float>(N, C) <= 227 * 1024 ? launch_cnn_t<float, false>(q, N, C, st)
                                               : launch_cnn_t<float, true>(q, N, C, st);

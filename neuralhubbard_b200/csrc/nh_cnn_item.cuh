@@ -41,15 +41,15 @@ __device__ __forceinline__ void cnn_lds8(const double* p, double* o) {
 // Builds the item's image configuration in simg (2N ints, +-1) and runs the layers; returns the
 // activation buffer (actA or actB) that holds the last layer's output, C planes of stride N + 1.
 // wsm: C * C * 9 values, bsm: C values (shared memory); actA, actB: C (N + 1) values each
-// (shared or per-block global memory).  Block-wide: every thread of the 256-thread block calls it.
-template <typename T>
+// (shared or per-block global memory).  Block-wide: every thread of the TH-thread block calls it.
+template <typename T, int TH = kNumThreads>
 __device__ T* cnn_layers(const float* __restrict__ wp, const float* __restrict__ bias, int Lx,
                          int Ly, int C, int layers, const int8_t* __restrict__ base, int fr,
                          int to, int g, T* actA, T* actB, T* wsm, T* bsm, int* simg) {
   const int tid = threadIdx.x;
   const int N = Lx * Ly, NS = N + 1, M2 = 2 * N;
   const int half = N / 2, ngroups = C / 8;
-  for (int m = tid; m < M2; m += kNumThreads) {
+  for (int m = tid; m < M2; m += TH) {
     const int src = sym_map(m, g, Lx, Ly, N);  // image[m] = s[g(m)] (g is an involution)
     const int v = move_value(src, base[src], fr, to);
     simg[m] = v > 0 ? 1 : -1;
@@ -63,11 +63,11 @@ __device__ T* cnn_layers(const float* __restrict__ wp, const float* __restrict__
   for (int l = 0; l < layers; ++l) {
     __syncthreads();
     const int cnt = C * cin * 9;
-    for (int i = tid; i < cnt; i += kNumThreads) wsm[i] = T(__ldg(wl + i));
-    for (int i = tid; i < C; i += kNumThreads) bsm[i] = T(__ldg(bias + l * C + i));
+    for (int i = tid; i < cnt; i += TH) wsm[i] = T(__ldg(wl + i));
+    for (int i = tid; i < C; i += TH) bsm[i] = T(__ldg(bias + l * C + i));
     __syncthreads();
     const bool act_fn = l < layers - 1;
-    for (int task = tid; task < ngroups * half; task += kNumThreads) {
+    for (int task = tid; task < ngroups * half; task += TH) {
       const int grp = task / half;
       const int s0 = task - grp * half, s1 = s0 + half;
       const int x0 = s0 / Ly, y0 = s0 - x0 * Ly;

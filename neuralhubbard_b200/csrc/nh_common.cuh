@@ -121,8 +121,9 @@ __device__ __forceinline__ int image_sign_parity(const int* simg, int g, int Lx,
                                  (int)(blockDim.x >> 5), BlockSync{});
 }
 
-// Exclusive scan of one int per thread over a kNumThreads block; returns the exclusive prefix,
-// *total the sum.  warp_buf: kNumThreads / 32 ints.
+// Exclusive scan of one int per thread over a TH-thread block (TH <= 1024); returns the exclusive
+// prefix, *total the sum.  warp_buf: TH / 32 ints.
+template <int TH = kNumThreads>
 __device__ __forceinline__ int block_scan(int v, int* warp_buf, int* total) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int x = v;
@@ -134,17 +135,17 @@ __device__ __forceinline__ int block_scan(int v, int* warp_buf, int* total) {
   if (lane == 31) warp_buf[wid] = x;
   __syncthreads();
   if (wid == 0) {
-    int w = lane < (kNumThreads / 32) ? warp_buf[lane] : 0;
+    int w = lane < (TH / 32) ? warp_buf[lane] : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       int y = __shfl_up_sync(0xffffffffu, w, o);
       if (lane >= o) w += y;
     }
-    if (lane < (kNumThreads / 32)) warp_buf[lane] = w;
+    if (lane < (TH / 32)) warp_buf[lane] = w;
   }
   __syncthreads();
   int base = wid ? warp_buf[wid - 1] : 0;
-  *total = warp_buf[kNumThreads / 32 - 1];
+  *total = warp_buf[TH / 32 - 1];
   __syncthreads();
   return base + x - v;
 }
@@ -162,34 +163,34 @@ __host__ __device__ __forceinline__ int swz_index(int r, int a) {
   return r * W + (((a / E) ^ swz_key(r, K)) * E) + (a % E);
 }
 
-// Mode-1 output of the backflow networks for one item, by a kNumThreads block: the ascending
+// Mode-1 output of the backflow networks for one item, by a TH-thread block: the ascending
 // occupied modes of the image configuration simg (+-1, 2N), the rows Y[p, a] = feat(spin, a,
 // site) of those modes (p < n), their mode indices, and the item sign eta_g(s) (-1)^(k(k-1)/2)
 // (0 for a wrong particle number k != n).  occl: 2N ints; wbuf: 4 Lx + 32 ints.
 // swizzle: rows in the chunk-swizzled layout of swz_index (shared-memory destinations).
-template <typename T, typename Feat>
+template <typename T, typename Feat, int TH = kNumThreads>
 __device__ void write_occupied_rows(const int* simg, int* occl, int* wbuf, int N, int n, int d,
                                     int g, int Lx, int Ly, T* Ydst, int32_t* idst,
                                     float* sign_dst, Feat feat, bool swizzle = false) {
   const int tid = threadIdx.x, M2 = 2 * N;
-  const int per = (M2 + kNumThreads - 1) / kNumThreads;
+  const int per = (M2 + TH - 1) / TH;
   const int m0 = tid * per;
   int cnt = 0;
   for (int m = m0; m < m0 + per && m < M2; ++m) cnt += simg[m] > 0;
   int total;
-  int pos = block_scan(cnt, wbuf, &total);
+  int pos = block_scan<TH>(cnt, wbuf, &total);
   for (int m = m0; m < m0 + per && m < M2; ++m)
     if (simg[m] > 0) occl[pos++] = m;
   __syncthreads();
   const int E = 16 / (int)sizeof(T), K = d / E;  // swizzled rows: K 16-byte chunks of E values
-  for (int o = tid; o < n * d; o += kNumThreads) {
+  for (int o = tid; o < n * d; o += TH) {
     const int p = o / d, aa = o - p * d;
     const int m = occl[p < total ? p : 0];
     const int sg = m >= N ? 1 : 0;
     const int dst = swizzle ? p * d + ((aa / E) ^ swz_key(p, K)) * E + aa % E : o;
     Ydst[dst] = feat(sg, aa, m - sg * N);
   }
-  for (int p = tid; p < n; p += kNumThreads) idst[p] = occl[p < total ? p : 0];
+  for (int p = tid; p < n; p += TH) idst[p] = occl[p < total ? p : 0];
   // eta_g from per-row occupation counts (closed form of the inversion parity).
   const int odd = image_sign_parity(simg, g, Lx, Ly, wbuf);
   if (tid == 0) {

@@ -89,7 +89,7 @@ struct Vec2<double> {
 // Phase 1: logical lower triangle A[p][q] = F[perm p][perm q] of one item into the CTA's slice
 // (element type T).  Warp <-> 32 consecutive logical columns q (their features in registers
 // when small), rows p > q in turn (the row's features broadcast); each element reads one Wt row.
-template <typename T, int D>
+template <typename T, int D, int kRegBytes = 64>
 __device__ void gather_permuted(const RefineArgs& a, const T* Yg, const int32_t* ig,
                                 const int* perm, unsigned char* smem, T* slice) {
   const int n = a.n, N = a.Lx * a.Ly;
@@ -137,7 +137,7 @@ __device__ void gather_permuted(const RefineArgs& a, const T* Yg, const int32_t*
   for (int qb = 0; 32 * qb + 1 < n; ++qb) total += n - 32 * qb - 1;
   int qb = 0, rem = wid, cur = -1, j = 0, infj = 0;
   // The column's features stay in registers when they are small, else they are read per element.
-  constexpr bool kRegs = D * sizeof(T) <= 64;
+  constexpr bool kRegs = D * sizeof(T) <= kRegBytes;
   T yj[kRegs ? D : 1];
 #pragma unroll 1
   for (int u = wid; u < total; u += kRWarps, rem += kRWarps) {
@@ -318,7 +318,8 @@ __global__ void __launch_bounds__(kRThreads, 1) refine_kernel(RefineArgs a) {
           Yg = sl;
           ig = reinterpret_cast<const int32_t*>(sl + n * D);
         }
-        gather_permuted<double, D>(a, Yg, ig, perm_s, smem, sl);
+        // mode 2 keeps each column's FP64 features in registers (its instance has the room)
+        gather_permuted<double, D, MODE == 2 ? 128 : 64>(a, Yg, ig, perm_s, smem, sl);
         __syncthreads();
         copy_slice(sl, S, tot);
       }
