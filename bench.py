@@ -23,7 +23,9 @@ against the library's all-FP64 path, and near-nodal log-Pfaffians at the slogpf 
 ``resconv`` (1 GPU) times the released states' residual network (16 blocks x 64 channels) on
 CUDA cores and on the tensor cores, with E/N of the released 16x16 state on 512 of its chains.
 ``extensions`` (1 GPU) times the per-sample Jacobian of log|psi_P|, the BCS-backflow ansatz (with
-its error against the BCS all-FP64 form) and the packed observables.
+its error against the BCS all-FP64 form) and the packed observables.  ``--config5`` (opt-in,
+several minutes) trains the learned proposal at 32x32 on records of plain chains and compares
+its tau_int and effective samples/s with the uniform hop there.
 
 Under torchrun each rank evaluates its own 8192 configurations (weak scaling); the time is the
 maximum over ranks of the summed per-step CUDA-event durations.  ``--impl reference`` times the
