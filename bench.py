@@ -547,7 +547,7 @@ def measure_precision(dev, st, spins, flush) -> dict:
     near = np.zeros(B, bool)
     near[nn_idx.cpu().numpy()] = True
     out["near-nodal slogpf, 8192 x 224x224 (1% seeded, pivot 1e-6)"] = {
-        "default (FP64 recompute of pivot ratio > 100)":
+        "default (FP64 refinement of pivot ratio > 5)":
             _err_stats(l1.cpu().numpy(), l0.cpu().numpy(), s1.cpu().numpy(), s0.cpu().numpy()),
         "FP32 only": _err_stats(l2.cpu().numpy(), l0.cpu().numpy(), s2.cpu().numpy(),
                                 s0.cpu().numpy()),
