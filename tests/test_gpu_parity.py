@@ -45,9 +45,9 @@ def rand_skew32(rng, n, batch):
 @pytest.mark.parametrize("n", [2, 4, 56, 100, 224, 236, 248, 256, 400, 1024])
 def test_slogpf_random(n):
     """Gaussian antisymmetric matrices (condition ~ n^2): plain FP32, and with the FP64
-    recompute of the matrices whose pivot ratio exceeds the default cond_tau (5).  Beyond shared memory (FP32
-    n > 256, FP64 n > 236) the triangles live in the workspace; cond_tau = 1 recomputes every
-    matrix in FP64."""
+    recompute of the matrices whose pivot ratio exceeds the default cond_tau (5).  Beyond shared
+    memory (FP32 n > 256, FP64 n > 236) the triangles live in the workspace; cond_tau = 1
+    recomputes every matrix in FP64."""
     rng = np.random.default_rng(n)
     A = rand_skew32(rng, n, 6 if n <= 400 else 3)
     s0, l0 = opf.slogpf(A.astype(np.float64))
