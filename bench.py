@@ -377,7 +377,7 @@ def measure_local_energy(args, dev, st) -> dict:
         model = nh.PfaffianBackflow(Lk, Lk, nek, nek, params=params, device=dev,
                                     cnn_mode=cnn_mode)
         state = nh.Variational(model, symm=False, max_parallel=8192)
-        B = args.eloc_samples if Lk <= 16 else min(args.eloc_samples, 256)
+        B = args.eloc_samples if Lk <= 16 else args.eloc_samples_large
         spins = torch.from_numpy(nh.random_spins(np.random.default_rng(500 + Lk), B, Nk, nek,
                                                  nek)).to(dev)
         psi = state(spins)
@@ -1368,6 +1368,8 @@ def main():
     ap.add_argument("--no-eloc", action="store_true",
                     help="skip the ragged local-energy measurement (8x8 and 16x16)")
     ap.add_argument("--eloc-samples", type=int, default=4096)
+    ap.add_argument("--eloc-samples-large", type=int, default=256,
+                    help="local-energy samples at 24x24 (4096 is config 4's size: ~6 minutes)")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the 32x32 (n = 896) Metropolis measurement")
     ap.add_argument("--large-chains", type=int, default=4096)
