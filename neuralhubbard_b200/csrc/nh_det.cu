@@ -9,9 +9,11 @@
 // 80-82).  One matrix per 512-thread CTA, held in registers: thread (warp w, lane c) owns rows
 // w + 16 t and columns c + 32 u.  Each thread gathers its own elements (features staged in shared
 // memory, Wt rows read through L1), then an LU elimination with implicit partial pivoting runs
-// on the registers: per step the column owners propose their largest unused entry (one 64-bit
-// shared-memory maximum), the pivot row goes through shared memory, and every unused row takes
-// its rank-1 update.  det F = parity(pivot order) x prod of the pivots; the log-sum of the
+// on the registers: per step each warp gathers column k of its rows onto its lanes by shuffles,
+// takes its largest unused entry with two 32-bit warp reductions, stores that row as its
+// candidate in shared memory and proposes it through one 64-bit shared-memory maximum; after the
+// step's one barrier every thread reads the winning warp's candidate as the pivot row, and every
+// unused row takes its rank-1 update.  det F = parity(pivot order) x prod of the pivots; the log-sum of the
 // pivots is accumulated in FP64 as mantissa and exponent.
 #include <math.h>
 
@@ -56,13 +58,13 @@ __global__ void __launch_bounds__(kDetThreads, 1) det_kernel(DetArgs a) {
   const int nh = a.nh, n = 2 * nh, N = a.Lx * a.Ly, Lx = a.Lx, Ly = a.Ly;
   T* ys = reinterpret_cast<T*>(smem_raw);          // (n, D)
   T* colbuf = ys + (size_t)n * D;                  // [2][NP]
-  T* rowbuf = colbuf + 2 * NP;                     // [2][NP]
-  T* pivs = rowbuf + 2 * NP;                       // [NP]
+  T* cand = colbuf + 2 * NP;                       // [2][16][NP] each warp's best row of the step
+  T* pivs = cand + 32 * NP;                        // [NP]
   int* info = reinterpret_cast<int*>(pivs + NP);   // (n) spin << 16 | x << 8 | y
   int* rho = info + n;                             // [NP] pivot row of step k
   int* mark = rho + NP;                            // [NP] parity scratch
-  unsigned long long* slot = reinterpret_cast<unsigned long long*>(mark + NP);  // [2]
-  int* bad_s = reinterpret_cast<int*>(slot + 2);
+  unsigned long long* slot = reinterpret_cast<unsigned long long*>(mark + NP);  // [3]
+  int* bad_s = reinterpret_cast<int*>(slot + 3);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T* Yb = static_cast<const T*>(a.Y);
   const T* Wud = static_cast<const T*>(a.Wt) + (size_t)N * D;
@@ -81,7 +83,7 @@ __global__ void __launch_bounds__(kDetThreads, 1) det_kernel(DetArgs a) {
       info[p] = (sp << 16) | (x << 8) | (site - x * Ly);
     }
     if (threadIdx.x == 0) {
-      slot[0] = slot[1] = 0ull;
+      slot[0] = slot[1] = 0ull;  // slot[2] is cleared after step 0's barrier
       *bad_s = 0;
     }
     __syncthreads();
@@ -117,27 +119,51 @@ __global__ void __launch_bounds__(kDetThreads, 1) det_kernel(DetArgs a) {
     for (int t = 0; t < TR; ++t)
       if (warp + 16 * t >= nh) used |= 1u << t;
     int bad = 0;
+    // One barrier per step.  The key slots rotate over three (slot sl is read after the step's
+    // barrier and cleared after the next step's barrier, two steps before its next use); the
+    // column and candidate buffers alternate by parity (a warp writes step k + 2's copy only
+    // after every warp has passed step k + 1's barrier, so after every read of step k's).
+    int sl = 0;
 #pragma unroll
     for (int uk = 0; uk < TC; ++uk) {
       for (int lk = 0; lk < 32; ++lk) {
         const int k = uk * 32 + lk;
         if (k >= nh || bad) break;  // uniform
         const int par = k & 1;
-        if (lane == lk) {
-          unsigned long long key = 0ull;
+        {
+          // Column k of this warp's rows, spread over the lanes (lane t takes row warp + 16 t)
+          // so that the pivot proposal runs on TR lanes instead of the one owning the column.
+          T cv = T(0);
 #pragma unroll
           for (int t = 0; t < TR; ++t) {
-            const T v = A[t][uk];
-            colbuf[par * NP + warp + 16 * t] = v;
-            if (!((used >> t) & 1u)) {
-              const unsigned long long kk = det_key(key_mag(v), warp + 16 * t);
-              key = kk > key ? kk : key;
-            }
+            const T v = __shfl_sync(0xffffffffu, A[t][uk], lk);
+            if (lane == t) cv = v;
           }
-          if (key) atomicMax(slot + par, key);
+          unsigned long long key = 0ull;
+          if (lane < TR) {
+            colbuf[par * NP + warp + 16 * lane] = cv;
+            if (!((used >> lane) & 1u)) key = det_key(key_mag(cv), warp + 16 * lane);
+          }
+          // 64-bit warp maximum as two 32-bit reductions: the magnitude bits, then the row
+          // tie-break among the lanes holding that magnitude.
+          const unsigned hi = (unsigned)(key >> 32);
+          const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+          const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? (unsigned)key : 0u);
+          key = ((unsigned long long)mh << 32) | ml;
+          if (key) {  // this warp's best row goes to its candidate slot
+            const int tl = (0x7FFFFFFF - (int)ml) >> 4;
+            T* cw = cand + (size_t)(par * 16 + warp) * NP;
+#pragma unroll
+            for (int t = 0; t < TR; ++t)
+              if (t == tl) {
+#pragma unroll
+                for (int u = 0; u < TC; ++u) cw[lane + 32 * u] = A[t][u];
+              }
+            if (lane == 0) atomicMax(slot + sl, key);
+          }
         }
         __syncthreads();
-        const unsigned long long win = slot[par];
+        const unsigned long long win = slot[sl];
         const int p = 0x7FFFFFFF - (int)(unsigned)(win & 0xFFFFFFFFull);
         const float mag = __uint_as_float((unsigned)(win >> 32));
         if (win == 0ull || !(mag > 0.0f && mag <= 3.0e38f)) {
@@ -145,26 +171,18 @@ __global__ void __launch_bounds__(kDetThreads, 1) det_kernel(DetArgs a) {
           __syncthreads();
           break;
         }
-        if (warp == (p & 15)) {
-          const int tp = p >> 4;
-#pragma unroll
-          for (int t = 0; t < TR; ++t)
-            if (t == tp) {
-#pragma unroll
-              for (int u = 0; u < TC; ++u) rowbuf[par * NP + lane + 32 * u] = A[t][u];
-              used |= 1u << t;
-            }
-        }
+        if (warp == (p & 15)) used |= 1u << (p >> 4);
         if (threadIdx.x == 0) {
-          slot[par ^ 1] = 0ull;
+          slot[sl == 0 ? 2 : sl - 1] = 0ull;
           rho[k] = p;
           pivs[k] = colbuf[par * NP + p];
         }
-        __syncthreads();
+        sl = sl == 2 ? 0 : sl + 1;
+        const T* prow = cand + (size_t)(par * 16 + (p & 15)) * NP;
         const T inv = T(1) / colbuf[par * NP + p];
         T r[TC];
 #pragma unroll
-        for (int u = 0; u < TC; ++u) r[u] = rowbuf[par * NP + lane + 32 * u] * inv;
+        for (int u = 0; u < TC; ++u) r[u] = prow[lane + 32 * u] * inv;
 #pragma unroll
         for (int t = 0; t < TR; ++t) {
           if ((used >> t) & 1u) continue;  // eliminated rows keep their values (never read)
@@ -230,7 +248,7 @@ template <typename T, int TC>
 size_t det_smem(int nh) {
   constexpr int NP = 32 * TC;
   const size_t n = 2 * (size_t)nh;
-  return sizeof(T) * (n * 16 + 5 * NP) + sizeof(int) * (n + 2 * NP) + 16 + 16;
+  return sizeof(T) * (n * 16 + 35 * NP) + sizeof(int) * (n + 2 * NP) + 24 + 16;
 }
 
 template <typename T, int TC>

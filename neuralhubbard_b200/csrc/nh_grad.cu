@@ -5,7 +5,8 @@
 // * adjoint_kernel: the cotangent of fermix.slogpf (code/backflow/models.py:210),
 //   G = d log|pf F| / dF = 1/2 F^{-T}, from an in-register Gauss-Jordan inverse of F with implicit
 //   row pivoting (one matrix per 512-thread CTA; thread (warp w, lane c) holds rows w + 16 t and
-//   columns c + 32 u).  A per-item scale multiplies G (the image weight of the projection).
+//   columns c + 32 u; one barrier per pivot step, the pivot row read from the winning warp's
+//   candidate row in shared memory, as in nh_det.cu).  A per-item scale multiplies G (the image weight of the projection).
 // * pairing_vjp_kernel: the custom VJP of the occupied gather (pf_kernel.py:193-320,354-365):
 //   dY[p, a] = sum_q (G - G^T)[p, q] Wt[blk(p, q), r(p, q), a] Y[q, a] and
 //   dWt[blk, r, a] = sum over the pairs (p, q) with that block and displacement of
@@ -59,18 +60,26 @@ struct AdjArgs {
   int32_t* flags;           // (batch,) or null: NH_FLAG_ZERO_PIVOT / NH_FLAG_NONFINITE
 };
 
+// Floats of the region shared by the output tile and the per-warp candidate rows.
+__host__ __device__ constexpr size_t adjoint_region(int n, int np) {
+  return (size_t)n * (n + 1) > (size_t)32 * np ? (size_t)n * (n + 1) : (size_t)32 * np;
+}
+
 template <int TC>
 __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjArgs a) {
   constexpr int TR = 2 * TC, NP = 32 * TC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = a.n, NS = n + 1;
-  float* tile = reinterpret_cast<float*>(smem_raw);  // (n, n + 1): G before the coalesced copy
-  float* colbuf = tile + (size_t)n * NS;              // [2][NP]
-  float* rowbuf = colbuf + 2 * NP;                    // [2][NP]
-  int* rho = reinterpret_cast<int*>(rowbuf + 2 * NP);  // [NP] pivot row of step k
+  // tile (n, n + 1): G before the coalesced copy.  During the elimination the same region holds
+  // cand [2][16][NP]: each warp's best remaining row of the step, so that the winner's row is
+  // in shared memory by the step's one barrier.
+  float* tile = reinterpret_cast<float*>(smem_raw);
+  float* cand = tile;
+  float* colbuf = tile + adjoint_region(n, NP);        // [2][NP]
+  int* rho = reinterpret_cast<int*>(colbuf + 2 * NP);  // [NP] pivot row of step k
   int* rhoinv = rho + NP;                              // [NP]
-  unsigned long long* slot = reinterpret_cast<unsigned long long*>(rhoinv + NP);  // [2]
-  float* scale_s = reinterpret_cast<float*>(slot + 2);
+  unsigned long long* slot = reinterpret_cast<unsigned long long*>(rhoinv + NP);  // [3]
+  float* scale_s = reinterpret_cast<float*>(slot + 3);
   int* bad_s = reinterpret_cast<int*>(scale_s + 1);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
@@ -91,7 +100,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjArgs a) {
     for (int t = 0; t < TR; ++t)
       if (warp + 16 * t >= n) used |= 1u << t;
     if (threadIdx.x == 0) {
-      slot[0] = slot[1] = 0ull;
+      slot[0] = slot[1] = 0ull;  // slot[2] is cleared after step 0's barrier
       *bad_s = 0;
       float sc = 0.5f;
       if (a.pf_sign) sc = (float)(0.5 * image_weight(a.pf_sign, a.pf_logabs, item, a.n_img));
@@ -99,27 +108,51 @@ __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjArgs a) {
     }
     __syncthreads();
     int bad = 0;
+    // One barrier per step.  The key slots rotate over three (slot sl is read after the step's
+    // barrier and cleared after the next step's barrier, two steps before its next use); the
+    // column and candidate buffers alternate by parity (a warp writes step k + 2's copy only
+    // after every warp has passed step k + 1's barrier, so after every read of step k's).
+    int sl = 0;
 #pragma unroll
     for (int uk = 0; uk < TC; ++uk) {
       for (int lk = 0; lk < 32; ++lk) {
         const int k = uk * 32 + lk;
         if (k >= n || bad) break;  // uniform
         const int par = k & 1;
-        if (lane == lk) {
-          unsigned long long key = 0ull;
+        {
+          // Column k of this warp's rows, spread over the lanes (lane t takes row warp + 16 t)
+          // so that the pivot proposal runs on TR lanes instead of the one owning the column.
+          float cv = float(0);
 #pragma unroll
           for (int t = 0; t < TR; ++t) {
-            const float v = A[t][uk];
-            colbuf[par * NP + warp + 16 * t] = v;
-            if (!((used >> t) & 1u)) {
-              const unsigned long long kk = pivot_key(fabsf(v), warp + 16 * t);
-              key = kk > key ? kk : key;
-            }
+            const float v = __shfl_sync(0xffffffffu, A[t][uk], lk);
+            if (lane == t) cv = v;
           }
-          if (key) atomicMax(slot + par, key);
+          unsigned long long key = 0ull;
+          if (lane < TR) {
+            colbuf[par * NP + warp + 16 * lane] = cv;
+            if (!((used >> lane) & 1u)) key = pivot_key(fabsf(cv), warp + 16 * lane);
+          }
+          // 64-bit warp maximum as two 32-bit reductions: the magnitude bits, then the row
+          // tie-break among the lanes holding that magnitude.
+          const unsigned hi = (unsigned)(key >> 32);
+          const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+          const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? (unsigned)key : 0u);
+          key = ((unsigned long long)mh << 32) | ml;
+          if (key) {  // this warp's best row goes to its candidate slot
+            const int tl = (0x7FFFFFFF - (int)ml) >> 4;
+            float* cw = cand + (size_t)(par * 16 + warp) * NP;
+#pragma unroll
+            for (int t = 0; t < TR; ++t)
+              if (t == tl) {
+#pragma unroll
+                for (int u = 0; u < TC; ++u) cw[lane + 32 * u] = A[t][u];
+              }
+            if (lane == 0) atomicMax(slot + sl, key);
+          }
         }
         __syncthreads();
-        const unsigned long long win = slot[par];
+        const unsigned long long win = slot[sl];
         const int p = 0x7FFFFFFF - (int)(unsigned)(win & 0xFFFFFFFFull);
         const float mag = __uint_as_float((unsigned)(win >> 32));
         if (win == 0ull || !(mag > 0.0f && mag <= 3.0e38f)) {  // zero column, or non-finite
@@ -127,25 +160,16 @@ __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjArgs a) {
           __syncthreads();
           break;
         }
-        if (warp == (p & 15)) {
-          const int tp = p >> 4;
-#pragma unroll
-          for (int t = 0; t < TR; ++t)
-            if (t == tp) {
-#pragma unroll
-              for (int u = 0; u < TC; ++u) rowbuf[par * NP + lane + 32 * u] = A[t][u];
-              used |= 1u << t;
-            }
-        }
         if (threadIdx.x == 0) {
-          slot[par ^ 1] = 0ull;
+          slot[sl == 0 ? 2 : sl - 1] = 0ull;
           rho[k] = p;
         }
-        __syncthreads();
-        const float inv = 1.0f / rowbuf[par * NP + k];
+        sl = sl == 2 ? 0 : sl + 1;
+        const float* prow = cand + (size_t)(par * 16 + (p & 15)) * NP;
+        const float inv = 1.0f / prow[k];
         float r[TC];
 #pragma unroll
-        for (int u = 0; u < TC; ++u) r[u] = rowbuf[par * NP + lane + 32 * u] * inv;
+        for (int u = 0; u < TC; ++u) r[u] = prow[lane + 32 * u] * inv;
 #pragma unroll
         for (int t = 0; t < TR; ++t) {
           const float f = colbuf[par * NP + warp + 16 * t];
@@ -158,6 +182,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjArgs a) {
         }
         if (warp == (p & 15)) {
           const int tp = p >> 4;
+          used |= 1u << tp;
 #pragma unroll
           for (int t = 0; t < TR; ++t)
             if (t == tp) {
@@ -204,8 +229,8 @@ __global__ void __launch_bounds__(kAdjThreads, 1) adjoint_kernel(AdjArgs a) {
 template <int TC>
 size_t adjoint_smem(int n) {
   constexpr int NP = 32 * TC;
-  return sizeof(float) * ((size_t)n * (n + 1) + 4 * NP) + sizeof(int) * 2 * NP +
-         sizeof(unsigned long long) * 2 + 16;
+  return sizeof(float) * (adjoint_region(n, NP) + 2 * NP) + sizeof(int) * 2 * NP +
+         sizeof(unsigned long long) * 3 + 16;
 }
 
 template <int TC>
