@@ -298,7 +298,9 @@ class BCSBackflow(PfaffianBackflow):
     (``bcs_kernel.py:1-70``; fd the nearest-neighbour d-wave form factor).  The features are the
     two spin halves of the backflow network's output (d = 16: 32 channels); parameters are those
     of ``PfaffianBackflow`` with W of shape (N, d) and ``delta_d`` (default 0.1, as
-    ``models.py:246``).  n_up == n_dn <= 224; FP64 recompute of flagged images up to 128."""
+    ``models.py:246``).  n_up == n_dn <= 224; FP64 recompute of flagged images up to 128.  The
+    reference's own BCS network (a learned (2, d, C) head on its ResConv trunk, d = 64,
+    ``models.py:262-265,330-331``) is not supported: the determinant's gather takes d = 16."""
 
     ansatz = _lib.ANSATZ_BCS
 
