@@ -300,7 +300,7 @@ class BCSBackflow(PfaffianBackflow):
     of ``PfaffianBackflow`` with W of shape (N, d) and ``delta_d`` (default 0.1, as
     ``models.py:246``).  n_up == n_dn <= 224; FP64 recompute of flagged images up to 128.  The
     reference's own BCS network (a learned (2, d, C) head on its ResConv trunk, d = 64,
-    ``models.py:262-265,330-331``) is not supported: the determinant's gather takes d = 16."""
+    ``models.py:261-270,330-331``) is not supported: the determinant's gather takes d = 16."""
 
     ansatz = _lib.ANSATZ_BCS
 
