@@ -6,10 +6,10 @@ block plus delta_d F^d, ``models.py:272-281``).
 
     python tests/golden/make_models_golden.py REFERENCE_ROOT
 
-The module is loaded as in ``make_pairing_golden.py`` (numpy in place of JAX), with empty
-stand-ins for the libraries it imports at module level (equinox, quantax, fermix): their names
-only have to exist for the module to load, and none of them is called by the functions run
-here.  The models are made with ``object.__new__`` and their fields set directly (no quantax
+The module is loaded as in ``make_pairing_golden.py`` (numpy in place of JAX where JAX is
+missing), with empty stand-ins for the libraries it imports at module level that are missing
+(equinox, quantax, fermix): their names only have to exist for the module to load, and none of
+them is called by the functions run here.  The models are made with ``object.__new__`` and their fields set directly (no quantax
 lattice); the Pfaffian model's network is the identity, so ``pairing_matrix(x)`` starts from a
 given network output x (2 d, LX, LY), and the BCS model's ``features`` returns the given (2, N, d)
 features.  Writes ``tests/golden/models_golden.npz``; for case k of CASES (LX, LY, d):
@@ -37,6 +37,11 @@ BATCH = 1
 
 
 def install_library_stand_ins():
+    import importlib.util
+
+    if all(importlib.util.find_spec(m) is not None for m in ("equinox", "quantax", "fermix")):
+        return
+
     class _Any(types.ModuleType):
         def __getattr__(self, name):
             return lambda *a, **k: None
@@ -75,25 +80,25 @@ def main(argv):
     for k, (LX, LY, d) in enumerate(CASES):
         N = LX * LY
         tables = models._einsum_tables(LX, LY)
+        # fields set with object.__setattr__: equinox modules are frozen dataclasses
         pf = object.__new__(models.PfaffianBackflow)
-        pf.net = lambda s: s
-        pf.d = d
-        pf.W = rng.normal(0.0, 0.5, size=(3, N, d))
-        pf.theta = np.float64(rng.normal(0.0, 0.5))
-        pf.geom = pfk.PairGeometry(LX, LY, d, 0, 0)
+        W, theta = rng.normal(0.0, 0.5, size=(3, N, d)), np.float64(rng.normal(0.0, 0.5))
+        for name, v in (("net", lambda s: s), ("d", d), ("W", W), ("theta", theta),
+                        ("geom", pfk.PairGeometry(LX, LY, d, 0, 0))):
+            object.__setattr__(pf, name, v)
         x = rng.normal(0.0, 1.0, size=(BATCH, 2 * d, LX, LY))
-        Fpf = np.stack([pf.pairing_matrix(x[b]) for b in range(BATCH)])
+        Fpf = np.stack([np.asarray(pf.pairing_matrix(x[b])) for b in range(BATCH)])
         bm = object.__new__(models.BCSBackflow)
-        bm.features = lambda s: s
-        bm.W = rng.normal(0.0, 0.5, size=(N, d))
-        bm.theta = np.float64(rng.normal(0.0, 0.5))
-        bm.delta_d = np.float64(rng.normal(0.0, 0.3))
-        bm.geom = bcs.UDGeometry(LX, LY, d, 0, 0)
+        Wb, thetab = rng.normal(0.0, 0.5, size=(N, d)), np.float64(rng.normal(0.0, 0.5))
+        delta = np.float64(rng.normal(0.0, 0.3))
+        for name, v in (("features", lambda s: s), ("W", Wb), ("theta", thetab),
+                        ("delta_d", delta), ("geom", bcs.UDGeometry(LX, LY, d, 0, 0))):
+            object.__setattr__(bm, name, v)
         y = rng.normal(0.0, 1.0, size=(BATCH, 2, N, d))
-        Fbcs = np.stack([bm.pairing_matrix(y[b]) for b in range(BATCH)])
+        Fbcs = np.stack([np.asarray(bm.pairing_matrix(y[b])) for b in range(BATCH)])
         out.update({f"dist_{k}": tables.dist, f"fd_{k}": tables.fd, f"x_{k}": x,
-                    f"W_{k}": pf.W, f"theta_{k}": pf.theta, f"Fpf_{k}": Fpf, f"y_{k}": y,
-                    f"Wb_{k}": bm.W, f"thetab_{k}": bm.theta, f"delta_{k}": bm.delta_d,
+                    f"W_{k}": W, f"theta_{k}": theta, f"Fpf_{k}": Fpf, f"y_{k}": y,
+                    f"Wb_{k}": Wb, f"thetab_{k}": thetab, f"delta_{k}": delta,
                     f"Fbcs_{k}": Fbcs})
     dst = os.path.join(HERE, "models_golden.npz")
     np.savez_compressed(dst, **out)

@@ -6,12 +6,13 @@ functions in ``code/backflow/pf_kernel.py`` (``displacement_tables``, ``build_wt
 
     python tests/golden/make_pairing_golden.py REFERENCE_ROOT
 
-JAX is not installed here, so the two modules are loaded with a stand-in ``jax`` module whose
-``jax.numpy`` is numpy (``einsum``'s ``precision`` argument dropped), ``jax.nn.softplus`` is
-log(1 + e^x) and ``jax.custom_vjp`` passes calls through; these reference functions use nothing
-else of JAX, so they run unchanged in FP64.  The package ``__init__`` (which imports equinox,
-quantax and fermix) is not executed.  Writes ``tests/golden/pairing_golden.npz``; for case k of
-CASES (LX, LY, d, n_up, n_dn), with seeded inputs stored beside the outputs:
+Where JAX is installed it is used, with 64-bit types enabled.  Where it is not, the two modules
+are loaded with a stand-in ``jax`` module whose ``jax.numpy`` is numpy (``einsum``'s
+``precision`` argument dropped), ``jax.nn.softplus`` is log(1 + e^x) and ``jax.custom_vjp``
+passes calls through; these reference functions use nothing else of JAX, so they run unchanged
+in FP64.  The package ``__init__`` (which imports equinox, quantax and fermix) is not executed.
+Writes ``tests/golden/pairing_golden.npz``; for case k of CASES (LX, LY, d, n_up, n_dn), with
+seeded inputs stored beside the outputs:
 
 * ``disp_k``, ``neg_k``, ``dist_k``: the displacement tables (``dist`` in FP32, as the
   reference stores it);
@@ -38,6 +39,12 @@ BATCH = 3
 
 
 def install_jax_stand_in():
+    if importlib.util.find_spec("jax") is not None:
+        import jax
+
+        jax.config.update("jax_enable_x64", True)
+        return
+
     class _NumpyAsJnp(types.ModuleType):
         def __getattr__(self, name):
             return getattr(np, name)
